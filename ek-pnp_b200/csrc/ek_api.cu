@@ -1,0 +1,508 @@
+// ek_api.cu -- the C ABI of libekpnp (declared in include/ekpnp.h).
+//
+// Host-side owner of a channel: allocation, parameter checks, the step loop
+// (one fused LBM launch + three Poisson launches per step) and field I/O.
+// Replaces the host code of main.cu:28-307 and the host wrappers of LBM.cu /
+// poisson.cu; every failure is returned as a status instead of exit().
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ek_internal.h"
+
+using namespace ek;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+    g_err = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? EK_ERR_NOMEM : EK_ERR_CUDA;
+}
+
+#define EK_CUDA(call, what)                              \
+    do {                                                 \
+        cudaError_t e_ = (call);                         \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+    } while (0)
+
+bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+}  // namespace
+
+struct ek_ctx {
+    ek_params p{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int nxp = 0, mp = 0, n = 0;
+    size_t plane = 0;
+    double *pops[2] = {nullptr, nullptr};
+    int cur = 0;
+    bool initialised = false;  // populations exist
+    bool state_pre = false;    // pops[cur] holds pre-collision populations in place
+    bool explicit_e_once = false;
+    bool e_stale = false;      // E planes older than psi
+    double *fields = nullptr;
+    double *wall = nullptr;    // 6 x nx
+    double *snap = nullptr;    // residual snapshot, 4 planes
+    double *part = nullptr;    // residual partial sums
+    bool snap_valid = false;
+    Rates *rates_dev = nullptr;
+    Rates rates{};
+    PoissonPlan pp{};
+    Chan chan{};
+    int64_t steps = 0;
+};
+
+namespace {
+
+int validate(const ek_params *p) {
+    if (!p) return fail(EK_ERR_INVALID, "null parameters");
+    if (p->nx < 2 || p->ny < 4) return fail(EK_ERR_INVALID, "need nx >= 2 and ny >= 4");
+    if (p->storage != EK_STORE_F64 && p->storage != EK_STORE_F32 && p->storage != EK_STORE_F16)
+        return fail(EK_ERR_INVALID, "unknown storage mode");
+    if (p->storage != EK_STORE_F64) return fail(EK_ERR_UNSUPPORTED, "storage mode not built yet");
+    if (is_pow2(p->nx) ? p->nx > 8192 : p->nx > 2048)
+        return fail(EK_ERR_UNSUPPORTED, "nx above 8192 (powers of two) or 2048 (other lengths)");
+    if (p->ny > 65535) return fail(EK_ERR_UNSUPPORTED, "ny above 65535");
+    const double pos[] = {p->dx, p->dy, p->dt, p->cfl, p->cs2, p->lx, p->nu, p->diff_p, p->diff_n,
+                          p->magic_f, p->magic_p, p->magic_n};
+    for (double v : pos)
+        if (!(v > 0.0) || !std::isfinite(v)) return fail(EK_ERR_INVALID, "non-positive or non-finite scale/rate parameter");
+    const double fin[] = {p->rho0, p->c0, p->mob_p, p->mob_n, p->eps, p->f_charge, p->zeta_lo,
+                          p->zeta_hi, p->cp_lo, p->cp_hi, p->cn_lo, p->cn_hi, p->ext_x, p->exf, p->uw};
+    for (double v : fin)
+        if (!std::isfinite(v)) return fail(EK_ERR_INVALID, "non-finite parameter");
+    if (p->eps == 0.0) return fail(EK_ERR_INVALID, "eps must be non-zero");
+    if (p->flags & ~(EK_FLAG_FORCE | EK_FLAG_REST_QUIRK | EK_FLAG_MOMENTS_EVERY_STEP | EK_FLAG_EXPLICIT_E))
+        return fail(EK_ERR_INVALID, "unknown flag bits");
+    return EK_OK;
+}
+
+void free_ctx(ek_ctx *c) {
+    if (!c) return;
+    cudaFree(c->pops[0]);
+    cudaFree(c->pops[1]);
+    cudaFree(c->fields);
+    cudaFree(c->wall);
+    cudaFree(c->snap);
+    cudaFree(c->part);
+    cudaFree(c->rates_dev);
+    cudaFree(c->pp.tw);
+    cudaFree(c->pp.piv);
+    cudaFree(c->pp.spec);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+// Pivots of the per-mode tridiagonal solve: b_m = -(2 + kx_m^2 dy^2),
+// kx_m = 2 pi m / Lx (main.cu:120-123); piv_0 = 1/b, piv_j = 1/(b - piv_{j-1}).
+std::vector<double> make_pivots(const ek_params &p, int n, int mp) {
+    std::vector<double> piv((size_t)n * mp, 0.0);
+    for (int m = 0; m <= p.nx / 2; ++m) {
+        const double kx = (double)m * 2.0 * M_PI / p.lx;
+        const double b = -(2.0 + kx * kx * p.dy * p.dy);
+        double c = 0.0;
+        for (int j = 0; j < n; ++j) {
+            c = 1.0 / (b - c);
+            piv[(size_t)j * mp + m] = c;
+        }
+    }
+    return piv;
+}
+
+std::vector<double2> make_twiddles(int nx) {
+    std::vector<double2> tw(nx);
+    for (int k = 0; k < nx; ++k) {
+        const long double a = 2.0L * 3.141592653589793238462643383279502884L * (long double)k / (long double)nx;
+        tw[k] = make_double2((double)cosl(a), (double)-sinl(a));
+    }
+    return tw;
+}
+
+void refresh_chan(ek_ctx *c) {
+    Chan &h = c->chan;
+    const ek_params &p = c->p;
+    h.nx = p.nx;
+    h.ny = p.ny;
+    h.nxp = c->nxp;
+    h.flags = p.flags;
+    h.plane = c->plane;
+    h.dx = p.dx;
+    h.dy = p.dy;
+    h.dt = p.dt;
+    h.cfl = p.cfl;
+    h.cs2 = p.cs2;
+    h.rho0 = p.rho0;
+    h.c0 = p.c0;
+    h.mob_p = p.mob_p;
+    h.mob_n = p.mob_n;
+    h.f_charge = p.f_charge;
+    h.eps = p.eps;
+    h.ext_x = p.ext_x;
+    h.exf = p.exf;
+    h.r = c->rates;
+    h.zlo = c->wall;
+    h.zhi = c->wall + p.nx;
+    h.cplo = c->wall + 2 * p.nx;
+    h.cphi = c->wall + 3 * p.nx;
+    h.cnlo = c->wall + 4 * p.nx;
+    h.cnhi = c->wall + 5 * p.nx;
+}
+
+int copy_in(ek_ctx *c, int plane_idx, const double *src) {
+    if (!src) return EK_OK;
+    const size_t w = (size_t)c->p.nx * sizeof(double);
+    EK_CUDA(cudaMemcpy2DAsync(c->fields + plane_idx * c->plane, (size_t)c->nxp * sizeof(double), src, w, w,
+                              c->p.ny, cudaMemcpyHostToDevice, c->stream),
+            "copy field to device");
+    return EK_OK;
+}
+
+int copy_out(ek_ctx *c, int plane_idx, double *dst, cudaMemcpyKind kind) {
+    if (!dst) return EK_OK;
+    const size_t w = (size_t)c->p.nx * sizeof(double);
+    EK_CUDA(cudaMemcpy2DAsync(dst, w, c->fields + plane_idx * c->plane, (size_t)c->nxp * sizeof(double), w,
+                              c->p.ny, kind, c->stream),
+            "copy field from device");
+    return EK_OK;
+}
+
+int refresh_e(ek_ctx *c) {
+    if (c->e_stale && !(c->p.flags & EK_FLAG_EXPLICIT_E)) {
+        EK_CUDA(launch_efield_f64(c->chan, c->fields, c->stream), "efield kernel");
+        c->e_stale = false;
+    }
+    return EK_OK;
+}
+
+int poisson_now(ek_ctx *c) {
+    EK_CUDA(poisson_solve_f64(c->pp, c->chan, c->fields, c->stream), "poisson kernels");
+    if (c->p.flags & EK_FLAG_EXPLICIT_E) {
+        EK_CUDA(launch_efield_f64(c->chan, c->fields, c->stream), "efield kernel");
+    } else {
+        c->e_stale = true;
+    }
+    return EK_OK;
+}
+
+}  // namespace
+
+// ---- residual kernels (ek_residual.cu) ----
+namespace ek {
+cudaError_t launch_residual_f64(const Chan &c, const double *fields, double *snap, double *part,
+                                int nblocks, double *out8, cudaStream_t s);
+int residual_blocks(const Chan &c);
+}  // namespace ek
+
+extern "C" {
+
+int ek_version(void) { return 100; }
+
+const char *ek_status_string(int status) {
+    switch (status) {
+        case EK_OK: return "ok";
+        case EK_ERR_INVALID: return "invalid argument";
+        case EK_ERR_CUDA: return "CUDA error";
+        case EK_ERR_NOMEM: return "out of device memory";
+        case EK_ERR_NAN: return "non-finite value in the solution";
+        case EK_ERR_TIMEOUT: return "bounded device wait timed out";
+        case EK_ERR_UNSUPPORTED: return "unsupported configuration";
+        case EK_ERR_TOO_LARGE: return "size above the call's maximum";
+        default: return "unknown status";
+    }
+}
+
+const char *ek_last_error(void) { return g_err.c_str(); }
+
+int ek_set_device(int32_t device) {
+    EK_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    return EK_OK;
+}
+
+int ek_get_device_count(int32_t *out) {
+    if (!out) return fail(EK_ERR_INVALID, "null argument");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        *out = 0;
+        return cuda_fail(e, "cudaGetDeviceCount");
+    }
+    *out = n;
+    return EK_OK;
+}
+
+int ek_params_default(ek_params *p, int32_t nx, int32_t ny) {
+    if (!p) return fail(EK_ERR_INVALID, "null parameters");
+    std::memset(p, 0, sizeof(*p));
+    p->nx = nx;
+    p->ny = ny;
+    p->storage = EK_STORE_F64;
+    p->flags = EK_FLAG_FORCE | EK_FLAG_REST_QUIRK;
+    p->dx = p->dy = p->dt = p->cfl = 1.0;
+    p->cs2 = 1.0 / 3.0;
+    p->lx = (double)nx;
+    p->rho0 = p->c0 = 1.0;
+    p->nu = 1.0 / 6.0;
+    p->magic_f = p->magic_p = p->magic_n = 0.25;
+    p->diff_p = p->diff_n = 0.05;
+    p->mob_p = 0.05;
+    p->mob_n = -0.05;
+    p->eps = 1.0;
+    p->f_charge = 1.0;
+    p->cp_lo = p->cp_hi = p->cn_lo = p->cn_hi = 1.0;
+    return EK_OK;
+}
+
+int ek_create(const ek_params *p, ek_ctx **out) {
+    if (!out) return fail(EK_ERR_INVALID, "null output pointer");
+    *out = nullptr;
+    int rc = validate(p);
+    if (rc != EK_OK) return rc;
+    ek_ctx *c = new ek_ctx();
+    c->p = *p;
+    cudaError_t e = cudaGetDevice(&c->device);
+    if (e != cudaSuccess) { free_ctx(c); return cuda_fail(e, "cudaGetDevice"); }
+    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { free_ctx(c); return cuda_fail(e, "stream create"); }
+    c->own_stream = true;
+    c->nxp = round_up(p->nx, 32);
+    c->plane = (size_t)p->ny * c->nxp;
+    c->n = p->ny - 2;
+    c->mp = round_up(p->nx / 2 + 1, 16);
+    const size_t pop_bytes = 27 * c->plane * sizeof(double);
+    struct Alloc { void **ptr; size_t bytes; } allocs[] = {
+        {(void **)&c->pops[0], pop_bytes},
+        {(void **)&c->pops[1], pop_bytes},
+        {(void **)&c->fields, F_COUNT * c->plane * sizeof(double)},
+        {(void **)&c->wall, 6 * (size_t)p->nx * sizeof(double)},
+        {(void **)&c->rates_dev, sizeof(Rates)},
+        {(void **)&c->pp.tw, (size_t)p->nx * sizeof(double2)},
+        {(void **)&c->pp.piv, (size_t)c->n * c->mp * sizeof(double)},
+        {(void **)&c->pp.spec, (size_t)c->n * c->mp * sizeof(double2)},
+    };
+    for (auto &a : allocs) {
+        e = cudaMalloc(a.ptr, a.bytes);
+        if (e == cudaSuccess) e = cudaMemsetAsync(*a.ptr, 0, a.bytes, c->stream);
+        if (e != cudaSuccess) { free_ctx(c); return cuda_fail(e, "device allocation"); }
+    }
+    // wall profiles start uniform
+    std::vector<double> wall(6 * (size_t)p->nx);
+    const double uni[6] = {p->zeta_lo, p->zeta_hi, p->cp_lo, p->cp_hi, p->cn_lo, p->cn_hi};
+    for (int k = 0; k < 6; ++k)
+        for (int x = 0; x < p->nx; ++x) wall[(size_t)k * p->nx + x] = uni[k];
+    std::vector<double> piv = make_pivots(*p, c->n, c->mp);
+    std::vector<double2> tw = make_twiddles(p->nx);
+    e = cudaMemcpyAsync(c->wall, wall.data(), wall.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->pp.piv, piv.data(), piv.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->pp.tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = launch_rates(*p, c->rates_dev, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&c->rates, c->rates_dev, sizeof(Rates), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e == cudaSuccess) e = poisson_set_smem_limits();
+    if (e != cudaSuccess) { free_ctx(c); return cuda_fail(e, "context set-up"); }
+    c->pp.nx = p->nx;
+    c->pp.ny = p->ny;
+    c->pp.n = c->n;
+    c->pp.mp = c->mp;
+    c->pp.pow2 = is_pow2(p->nx);
+    int lg = 0;
+    while ((1 << lg) < p->nx) ++lg;
+    c->pp.log2nx = c->pp.pow2 ? lg : 0;
+    c->pp.dy2 = p->dy * p->dy;
+    refresh_chan(c);
+    *out = c;
+    return EK_OK;
+}
+
+int ek_destroy(ek_ctx *c) {
+    if (!c) return fail(EK_ERR_INVALID, "null context");
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    free_ctx(c);
+    return EK_OK;
+}
+
+int ek_set_stream(ek_ctx *c, void *stream) {
+    if (!c) return fail(EK_ERR_INVALID, "null context");
+    EK_CUDA(cudaStreamSynchronize(c->stream), "stream sync");
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    c->stream = (cudaStream_t)stream;
+    c->own_stream = false;
+    return EK_OK;
+}
+
+int ek_get_params(const ek_ctx *c, ek_params *out) {
+    if (!c || !out) return fail(EK_ERR_INVALID, "null argument");
+    *out = c->p;
+    return EK_OK;
+}
+
+int ek_set_fields(ek_ctx *c, const double *rho, const double *ux, const double *uy, const double *cp,
+                  const double *cn, const double *psi, const double *ex, const double *ey) {
+    if (!c) return fail(EK_ERR_INVALID, "null context");
+    if ((ex == nullptr) != (ey == nullptr)) return fail(EK_ERR_INVALID, "give both ex and ey, or neither");
+    const double *src[F_RHS] = {rho, ux, uy, cp, cn, psi, ex, ey};
+    for (int k = 0; k < F_RHS; ++k) {
+        int rc = copy_in(c, k, src[k]);
+        if (rc != EK_OK) return rc;
+    }
+    if (ex) {
+        c->explicit_e_once = true;
+        c->e_stale = false;
+    } else if (psi) {
+        c->e_stale = true;
+    }
+    EK_CUDA(cudaStreamSynchronize(c->stream), "set_fields sync");
+    return EK_OK;
+}
+
+int ek_set_wall_profile(ek_ctx *c, const double *zlo, const double *zhi, const double *cplo,
+                        const double *cphi, const double *cnlo, const double *cnhi) {
+    if (!c) return fail(EK_ERR_INVALID, "null context");
+    const double *src[6] = {zlo, zhi, cplo, cphi, cnlo, cnhi};
+    for (int k = 0; k < 6; ++k) {
+        if (!src[k]) continue;
+        for (int x = 0; x < c->p.nx; ++x)
+            if (!std::isfinite(src[k][x])) return fail(EK_ERR_INVALID, "non-finite wall value");
+        EK_CUDA(cudaMemcpyAsync(c->wall + (size_t)k * c->p.nx, src[k], c->p.nx * sizeof(double),
+                                cudaMemcpyHostToDevice, c->stream),
+                "copy wall profile");
+    }
+    EK_CUDA(cudaStreamSynchronize(c->stream), "wall profile sync");
+    return EK_OK;
+}
+
+int ek_init_equilibrium(ek_ctx *c) {
+    if (!c) return fail(EK_ERR_INVALID, "null context");
+    const bool ee = c->explicit_e_once || (c->p.flags & EK_FLAG_EXPLICIT_E);
+    EK_CUDA(launch_init_f64(c->chan, c->pops[c->cur], c->fields, ee, c->stream), "init kernel");
+    c->initialised = true;
+    c->state_pre = true;
+    c->steps = 0;
+    c->snap_valid = false;
+    return EK_OK;
+}
+
+int ek_step(ek_ctx *c, int32_t nsteps) {
+    if (!c || nsteps < 0) return fail(EK_ERR_INVALID, "null context or negative step count");
+    if (!c->initialised) return fail(EK_ERR_INVALID, "call ek_init_equilibrium before ek_step");
+    const bool every = (c->p.flags & EK_FLAG_MOMENTS_EVERY_STEP) != 0;
+    for (int32_t i = 0; i < nsteps; ++i) {
+        const bool ee = c->explicit_e_once || (c->p.flags & EK_FLAG_EXPLICIT_E);
+        EK_CUDA(launch_step_f64(c->chan, c->pops[c->cur], c->pops[c->cur ^ 1], c->fields, c->state_pre, ee,
+                                every || i == nsteps - 1, c->stream),
+                "LBM step kernel");
+        c->cur ^= 1;
+        c->state_pre = false;
+        c->explicit_e_once = false;
+        int rc = poisson_now(c);
+        if (rc != EK_OK) return rc;
+        ++c->steps;
+    }
+    return EK_OK;
+}
+
+int ek_poisson(ek_ctx *c) {
+    if (!c) return fail(EK_ERR_INVALID, "null context");
+    EK_CUDA(launch_rhs_from_moments_f64(c->chan, c->fields, c->stream), "rhs kernel");
+    return poisson_now(c);
+}
+
+int ek_get_fields(ek_ctx *c, double *rho, double *ux, double *uy, double *cp, double *cn, double *psi,
+                  double *ex, double *ey) {
+    if (!c) return fail(EK_ERR_INVALID, "null context");
+    if (ex || ey) {
+        int rc = refresh_e(c);
+        if (rc != EK_OK) return rc;
+    }
+    double *dst[F_RHS] = {rho, ux, uy, cp, cn, psi, ex, ey};
+    for (int k = 0; k < F_RHS; ++k) {
+        int rc = copy_out(c, k, dst[k], cudaMemcpyDeviceToHost);
+        if (rc != EK_OK) return rc;
+    }
+    EK_CUDA(cudaStreamSynchronize(c->stream), "get_fields sync");
+    return EK_OK;
+}
+
+int ek_get_fields_device(ek_ctx *c, double *rho, double *ux, double *uy, double *cp, double *cn,
+                         double *psi, double *ex, double *ey) {
+    if (!c) return fail(EK_ERR_INVALID, "null context");
+    if (ex || ey) {
+        int rc = refresh_e(c);
+        if (rc != EK_OK) return rc;
+    }
+    double *dst[F_RHS] = {rho, ux, uy, cp, cn, psi, ex, ey};
+    for (int k = 0; k < F_RHS; ++k) {
+        int rc = copy_out(c, k, dst[k], cudaMemcpyDeviceToDevice);
+        if (rc != EK_OK) return rc;
+    }
+    return EK_OK;
+}
+
+int ek_residual(ek_ctx *c, int32_t interval, double *out5) {
+    if (!c || !out5 || interval <= 0) return fail(EK_ERR_INVALID, "bad residual arguments");
+    if (!c->snap) {
+        EK_CUDA(cudaMalloc(&c->snap, 4 * c->plane * sizeof(double)), "residual snapshot");
+        EK_CUDA(cudaMemsetAsync(c->snap, 0, 4 * c->plane * sizeof(double), c->stream), "residual snapshot");
+        EK_CUDA(cudaMalloc(&c->part, (size_t)residual_blocks(c->chan) * 8 * sizeof(double) + 8 * sizeof(double)),
+                "residual partials");
+    }
+    double sums[8];
+    const int nb = residual_blocks(c->chan);
+    EK_CUDA(launch_residual_f64(c->chan, c->fields, c->snap, c->part, nb, c->part + (size_t)nb * 8, c->stream),
+            "residual kernels");
+    EK_CUDA(cudaMemcpyAsync(sums, c->part + (size_t)nb * 8, sizeof(sums), cudaMemcpyDeviceToHost, c->stream),
+            "residual copy");
+    EK_CUDA(cudaStreamSynchronize(c->stream), "residual sync");
+    for (double v : sums)
+        if (!std::isfinite(v)) return fail(EK_ERR_NAN, "non-finite value in ux, c+, c- or psi");
+    const bool had = c->snap_valid;
+    c->snap_valid = true;
+    const double nn = (double)c->p.nx * (double)c->p.ny;
+    // u_x is normalised by at least the Helmholtz-Smoluchowski speed |eps zeta E/(rho nu)|
+    const double uhs = std::fabs(c->p.eps * c->p.zeta_lo * c->p.ext_x / (c->p.rho0 * c->p.nu));
+    const double floors[4] = {std::max(uhs * std::sqrt(nn), 1e-300), 1e-300, 1e-300, 1e-300};
+    double worst = 0.0;
+    for (int q = 0; q < 4; ++q) {
+        const double norm = std::max(std::sqrt(sums[4 + q]), floors[q]);
+        out5[q] = had ? std::sqrt(sums[q]) / ((double)interval * norm) : INFINITY;
+        worst = std::max(worst, out5[q]);
+    }
+    out5[4] = worst;
+    return EK_OK;
+}
+
+int ek_step_count(const ek_ctx *c, int64_t *out) {
+    if (!c || !out) return fail(EK_ERR_INVALID, "null argument");
+    *out = c->steps;
+    return EK_OK;
+}
+
+int ek_sync(ek_ctx *c) {
+    if (!c) return fail(EK_ERR_INVALID, "null context");
+    EK_CUDA(cudaStreamSynchronize(c->stream), "sync");
+    return EK_OK;
+}
+
+int ek_field_pointers(ek_ctx *c, double **out8, int32_t *pitch) {
+    if (!c || !out8) return fail(EK_ERR_INVALID, "null argument");
+    if (pitch) *pitch = c->nxp;
+    int rc = refresh_e(c);
+    if (rc != EK_OK) return rc;
+    for (int k = 0; k < F_RHS; ++k) out8[k] = c->fields + k * c->plane;
+    return EK_OK;
+}
+
+}  // extern "C"

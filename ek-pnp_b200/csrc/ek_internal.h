@@ -1,0 +1,80 @@
+// ek_internal.h -- shared definitions of libekpnp's kernels and C ABI.
+//
+// Device memory of one channel (all planes ny rows x nxp columns, nxp = nx
+// rounded up to 32 so every row starts 256-byte aligned):
+//   pops[2]   27 planes each, ping-pong: species-major (fluid f, c+ h, c- t),
+//             then direction 0..8 in the reference numbering (LBM.cu:831-834).
+//             Between steps a buffer holds POST-collision populations; the next
+//             step pulls them (streaming fused into the load).  Right after
+//             ek_init_equilibrium it holds pre-collision populations at their
+//             own node ("state_pre"), and the first step reads them in place.
+//   fields    9 planes: rho, ux, uy, c+, c-, psi, Ex, Ey, and the Poisson
+//             right-hand side.
+//   spec      (ny-2) x mp complex: x-spectrum of the interior rows (mp >= nx/2+1)
+//   piv       (ny-2) x mp: pivots of the per-mode tridiagonal y-solve
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/ekpnp.h"
+
+namespace ek {
+
+// D2Q9 velocity set in the reference numbering:  6 2 5 / 3 0 1 / 7 4 8
+__host__ __device__ constexpr int cxd(int d) {
+    return d == 1 || d == 5 || d == 8 ? 1 : (d == 3 || d == 6 || d == 7 ? -1 : 0);
+}
+__host__ __device__ constexpr int cyd(int d) {
+    return d == 2 || d == 5 || d == 6 ? 1 : (d == 4 || d == 7 || d == 8 ? -1 : 0);
+}
+__host__ __device__ constexpr int oppd(int d) { return d == 0 ? 0 : (d <= 4 ? (d + 1) % 4 + 1 : (d - 3) % 4 + 5); }
+static_assert(oppd(1) == 3 && oppd(2) == 4 && oppd(3) == 1 && oppd(4) == 2, "opp straight");
+static_assert(oppd(5) == 7 && oppd(6) == 8 && oppd(7) == 5 && oppd(8) == 6, "opp diagonal");
+
+constexpr double W0 = 4.0 / 9.0, WS = 1.0 / 9.0, WD = 1.0 / 36.0;  // LBM.h:105-107
+
+// Relaxation and wall constants, evaluated on the device with the reference's
+// expressions (LBM.cu:336-341, 745-746, 812-813) so they round as it does.
+struct Rates {
+    double wp, wm;    // fluid omega+*dt, omega-*dt
+    double wcp, wcm;  // c+  (minus set by diffu, plus by VC)
+    double wtp, wtm;  // c-  (minus set by D, plus by VT)
+    double sp, sm;    // Guo source factors 1 - dt*omega/2
+    double ms, md;    // moving top wall terms
+};
+
+// Per-channel constants, passed by value to every kernel.
+struct Chan {
+    int nx, ny, nxp, flags;
+    size_t plane;  // ny * nxp
+    double dx, dy, dt, cfl, cs2, rho0, c0;
+    double mob_p, mob_n, f_charge, eps, ext_x, exf;
+    Rates r;
+    const double *zlo, *zhi, *cplo, *cphi, *cnlo, *cnhi;  // per-x wall values (nx each)
+};
+
+enum Field { F_RHO = 0, F_UX, F_UY, F_CP, F_CN, F_PSI, F_EX, F_EY, F_RHS, F_COUNT };
+
+// ---- launchers (ek_lbm_f64.cu) ----
+cudaError_t launch_rates(const ek_params &p, Rates *dev_out, cudaStream_t s);
+cudaError_t launch_init_f64(const Chan &c, double *pops, const double *fields, bool explicit_e,
+                            cudaStream_t s);
+cudaError_t launch_step_f64(const Chan &c, const double *src, double *dst, double *fields,
+                            bool first, bool explicit_e, bool moments, cudaStream_t s);
+cudaError_t launch_efield_f64(const Chan &c, double *fields, cudaStream_t s);
+cudaError_t launch_rhs_from_moments_f64(const Chan &c, double *fields, cudaStream_t s);
+
+// ---- Poisson (ek_poisson.cu) ----
+struct PoissonPlan {
+    int nx, ny, n, mp, log2nx;  // n = ny-2 interior rows
+    bool pow2;
+    double dy2;                 // dy*dy
+    double2 *tw;                // nx twiddles exp(-2 pi i k/nx)
+    double *piv;                // n x mp pivots
+    double2 *spec;              // n x mp spectrum
+};
+cudaError_t poisson_solve_f64(const PoissonPlan &pp, const Chan &c, double *fields, cudaStream_t s);
+size_t poisson_smem_bytes_f64(int nx);
+cudaError_t poisson_set_smem_limits();
+
+}  // namespace ek

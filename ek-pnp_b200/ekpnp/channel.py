@@ -1,0 +1,120 @@
+"""Host-side channel object over the C ABI.
+
+Mirrors the reference's host entry points (LBM.h:149-169) for one channel:
+    read_data          -> Channel.set_fields            (LBM.cu:1350-1391)
+    init_equilibrium   -> Channel.init_equilibrium      (LBM.cu:183-193)
+    stream_collide_save + fast_Poisson (one loop body of main.cu:190-233)
+                       -> Channel.step(1)
+    fast_Poisson       -> Channel.poisson               (poisson.cu:180-208)
+Errors raise EkError with the library's status instead of exiting.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import EkParams, check, lib
+
+FIELD_NAMES = ("rho", "ux", "uy", "cp", "cn", "psi", "ex", "ey")
+
+
+def set_device(device: int):
+    check(lib().ek_set_device(int(device)))
+
+
+def device_count() -> int:
+    n = ctypes.c_int32(0)
+    rc = lib().ek_get_device_count(ctypes.byref(n))
+    return int(n.value) if rc == _lib.EK_OK else 0
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Channel:
+    def __init__(self, params):
+        self.params = dict(params) if not isinstance(params, EkParams) else params.to_dict()
+        self._p = EkParams.from_dict(self.params)
+        self.nx, self.ny = int(self._p.nx), int(self._p.ny)
+        h = ctypes.c_void_p()
+        check(lib().ek_create(ctypes.byref(self._p), ctypes.byref(h)))
+        self._h = h
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            check(lib().ek_destroy(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- state ------------------------------------------------------------
+    def _arr(self, a):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        if a.shape != (self.ny, self.nx):
+            raise ValueError(f"field shape {a.shape} != {(self.ny, self.nx)}")
+        return a
+
+    def set_fields(self, rho=None, ux=None, uy=None, cp=None, cn=None, psi=None, ex=None, ey=None):
+        arrs = [self._arr(a) for a in (rho, ux, uy, cp, cn, psi, ex, ey)]
+        check(lib().ek_set_fields(self._h, *[_ptr(a) for a in arrs]))
+
+    read_data = set_fields
+
+    def set_wall_profile(self, zeta_lo=None, zeta_hi=None, cp_lo=None, cp_hi=None, cn_lo=None, cn_hi=None):
+        arrs = []
+        for a in (zeta_lo, zeta_hi, cp_lo, cp_hi, cn_lo, cn_hi):
+            if a is not None:
+                a = np.ascontiguousarray(a, dtype=np.float64)
+                if a.shape != (self.nx,):
+                    raise ValueError("wall profiles have nx entries")
+            arrs.append(a)
+        check(lib().ek_set_wall_profile(self._h, *[_ptr(a) for a in arrs]))
+
+    def init_equilibrium(self):
+        check(lib().ek_init_equilibrium(self._h))
+
+    def step(self, n=1):
+        check(lib().ek_step(self._h, int(n)))
+
+    def poisson(self):
+        check(lib().ek_poisson(self._h))
+
+    fast_Poisson = poisson
+
+    def sync(self):
+        check(lib().ek_sync(self._h))
+
+    def get_fields(self, names=FIELD_NAMES):
+        out = {n: np.empty((self.ny, self.nx)) for n in names}
+        check(lib().ek_get_fields(self._h, *[_ptr(out.get(n)) for n in FIELD_NAMES]))
+        return out
+
+    def residual(self, interval):
+        out = np.empty(5)
+        check(lib().ek_residual(self._h, int(interval), _ptr(out)))
+        return out
+
+    @property
+    def steps(self):
+        v = ctypes.c_int64()
+        check(lib().ek_step_count(self._h, ctypes.byref(v)))
+        return int(v.value)
+
+    def set_stream(self, stream_handle: int):
+        check(lib().ek_set_stream(self._h, ctypes.c_void_p(stream_handle)))

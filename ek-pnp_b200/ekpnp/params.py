@@ -1,0 +1,66 @@
+"""Channel parameters in lattice units and the benchmark workloads.
+
+Mapping of the reference's SI constants (LBM.h:39-112) to lattice units:
+  dx = dy = dt = CFL = 1, cs_square = 1/3, Lx = nx, H = ny-1 (wall row to
+  wall row, the Dirichlet rows of the Poisson solve)
+  nu = cs2*(tau_s - 1/2); V = VC = VT = Lambda (TRT magic parameter)
+  diffu = D for both ions; mobility K = +D, Kn = -D (potential in thermal
+  volts, e/kT = 1)
+  eps = 1 and convertCtoCharge = eps*kappa^2/(2*c0), kappa = kappaH/H, so the
+  linearised Poisson-Boltzmann equation reads lap(psi) = kappa^2 psi
+  voltage = voltage2 = zeta; wall c+ = c0*exp(-zeta), wall c- = c0*exp(+zeta)
+  Ext = E_x, exf = 0, uw = 0, rho0 = 1.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from ._lib import FLAG_FORCE, FLAG_REST_QUIRK, STORE_F64
+
+
+def channel_params(nx, ny, *, kappa_h=8.0, zeta=-2.0, ex=1e-4, diff=0.05, tau_s=1.0, magic=0.25,
+                   c0=1.0, rho0=1.0, eps=1.0, storage=STORE_F64, force=True, rest_quirk=True,
+                   zeta_hi=None, uw=0.0, extra_flags=0):
+    zeta_hi = zeta if zeta_hi is None else zeta_hi
+    cs2 = 1.0 / 3.0
+    kappa = kappa_h / (ny - 1)
+    flags = (FLAG_FORCE if force else 0) | (FLAG_REST_QUIRK if rest_quirk else 0) | extra_flags
+    return dict(
+        nx=int(nx), ny=int(ny), storage=int(storage), flags=int(flags),
+        dx=1.0, dy=1.0, dt=1.0, cfl=1.0, cs2=cs2, lx=float(nx), rho0=rho0, c0=c0,
+        nu=cs2 * (tau_s - 0.5), magic_f=magic, diff_p=diff, magic_p=magic, mob_p=diff,
+        diff_n=diff, magic_n=magic, mob_n=-diff, eps=eps, f_charge=eps * kappa * kappa / (2.0 * c0),
+        zeta_lo=zeta, zeta_hi=zeta_hi, cp_lo=c0 * math.exp(-zeta), cp_hi=c0 * math.exp(-zeta_hi),
+        cn_lo=c0 * math.exp(zeta), cn_hi=c0 * math.exp(zeta_hi), ext_x=ex, exf=0.0, uw=uw)
+
+
+def helmholtz_smoluchowski(p):
+    """Plug velocity u_HS = -eps*zeta*E/(rho0*nu) of a thin double layer."""
+    return -p["eps"] * p["zeta_lo"] * p["ext_x"] / (p["rho0"] * p["nu"])
+
+
+def noisy_uniform_state(nx, ny, seed, c0=1.0, rho0=1.0, noise=1e-3):
+    """u = 0, psi = 0, rho = rho0, c+- = c0*(1 + noise*N(0,1)); numpy
+    default_rng(seed), standard normals of shape (ny, nx) drawn for c+ then c-."""
+    rng = np.random.default_rng(seed)
+    cp = c0 * (1.0 + noise * rng.standard_normal((ny, nx)))
+    cn = c0 * (1.0 + noise * rng.standard_normal((ny, nx)))
+    z = np.zeros((ny, nx))
+    return dict(rho=np.full((ny, nx), rho0), ux=z.copy(), uy=z.copy(), cp=cp, cn=cn, psi=z.copy(),
+                ex=z.copy(), ey=z.copy())
+
+
+# Benchmark channels: the single channels of the workload set.
+WORKLOADS = {
+    "channel-256x128": dict(nx=256, ny=128, kappa_h=8.0, zeta=-2.0, ex=1e-4, diff=0.05, seed=0, steps=20000),
+    "channel-4096x1024": dict(nx=4096, ny=1024, kappa_h=32.0, zeta=-4.0, ex=5e-5, diff=0.05, seed=1, steps=10000),
+    "channel-8192x2048": dict(nx=8192, ny=2048, kappa_h=64.0, zeta=-2.0, ex=1e-4, diff=0.05, seed=5, steps=0),
+}
+
+
+def workload_params(name, storage=STORE_F64, extra_flags=0):
+    w = WORKLOADS[name]
+    return channel_params(w["nx"], w["ny"], kappa_h=w["kappa_h"], zeta=w["zeta"], ex=w["ex"],
+                          diff=w["diff"], storage=storage, extra_flags=extra_flags)

@@ -1,0 +1,191 @@
+/*
+ * ekpnp.h -- C ABI of the B200 EK-PNP channel solver (libekpnp.so).
+ *
+ * One solver context ("channel") holds a 2D channel of nx*ny lattice nodes,
+ * periodic in x, with walls at y = 0 and y = ny-1.  Each time step is the
+ * coupled update of the reference code (gyf135/EK-PNP):
+ *   - TRT D2Q9 fluid with Guo forcing by the electric body force,
+ *   - TRT D2Q9 Nernst-Planck populations for c+ and c-,
+ *   - wall boundary conditions (fluid full-way bounce-back, ion Dirichlet
+ *     anti-bounce-back),
+ *   - spectral Poisson solve for the potential psi and the field E = -grad psi.
+ *
+ * Every entry point returns an int status (EK_OK = 0, see ek_status_string)
+ * instead of calling exit() as the reference does (LBM.cu:44-62, LBM.h:182-203).
+ * All field arrays are row-major nx*ny doubles, index = nx*y + x, the
+ * reference's scalar_index (LBM.h:172-175).  Pointers are host pointers unless
+ * the call says otherwise.  No torch or CUDA types appear in the signatures;
+ * streams are passed as void* (a cudaStream_t).
+ */
+#ifndef EKPNP_H
+#define EKPNP_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+enum {
+    EK_OK = 0,
+    EK_ERR_INVALID = 1,     /* bad argument or parameter (rejected on the host) */
+    EK_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+    EK_ERR_NOMEM = 3,       /* device allocation failed */
+    EK_ERR_NAN = 4,         /* non-finite value found by a residual/health reduction */
+    EK_ERR_TIMEOUT = 5,     /* a bounded device wait gave up (batched work queue) */
+    EK_ERR_UNSUPPORTED = 6, /* configuration outside what this build supports */
+    EK_ERR_TOO_LARGE = 7    /* size above the documented maximum of the call */
+};
+
+/* ---- population storage ---------------------------------------------- */
+enum {
+    EK_STORE_F64 = 0,       /* FP64 populations, reference arithmetic order      */
+    EK_STORE_F32 = 1,       /* FP32 deviations f - w_i*rho0, h - w_i*c0          */
+    EK_STORE_F16 = 2        /* FP16 deviations, FP32 arithmetic                  */
+};
+
+/* ---- behaviour flags (ek_params.flags) --------------------------------- */
+enum {
+    /* Electric body force on the fluid, F = f_charge*(c+ - c-)*(E + ext_x) + exf.
+     * The reference ships it commented out (LBM.cu:388-389, 438-439); set this
+     * to run the driven flow the commented expression describes. */
+    EK_FLAG_FORCE = 1 << 0,
+    /* Negative-ion rest equilibrium uses the fluid's 1 - u^2/(2cs^2) instead
+     * of the c- drift velocity, as gpu_collide_save does (LBM.cu:493).  Off
+     * gives the consistent form used by gpu_init_equilibrium (LBM.cu:242). */
+    EK_FLAG_REST_QUIRK = 1 << 1,
+    /* Write rho, ux, uy, c+, c- of every step to the context's field buffers
+     * (the reference writes them every step, LBM.cu:447-451).  Without it they
+     * are written only on the steps that need them (residual, ek_get_fields). */
+    EK_FLAG_MOMENTS_EVERY_STEP = 1 << 2,
+    /* Keep explicit Ex/Ey arrays written by the Poisson step and read by the
+     * collision (reference data flow, poisson.cu:132-174).  Without it the
+     * collision differentiates psi itself with the same stencil. */
+    EK_FLAG_EXPLICIT_E = 1 << 3
+};
+
+/* Physical and numerical constants of one channel.  Names follow the
+ * reference's LBM.h symbols (cited per field); any consistent unit system
+ * works, lattice units being dx = dy = dt = cfl = 1, cs2 = 1/3. */
+typedef struct ek_params {
+    int32_t nx;          /* NX (LBM.h:35); x is periodic                       */
+    int32_t ny;          /* NY (LBM.h:36); walls at y = 0 and ny-1, ny >= 4    */
+    int32_t storage;     /* EK_STORE_*                                         */
+    int32_t flags;       /* EK_FLAG_*                                          */
+    double dx, dy;       /* dx, dy (LBM.h:42-43)                               */
+    double dt;           /* dt (LBM.h:51)                                      */
+    double cfl;          /* CFL = dt/dx (LBM.h:50)                             */
+    double cs2;          /* cs_square (LBM.h:52)                               */
+    double lx;           /* Lx, x period of the spectral symbol (LBM.h:40)     */
+    double rho0;         /* rho0 (LBM.h:53); fluid shift of the FP32/16 forms  */
+    double c0;           /* bulk concentration; ion shift of the FP32/16 forms */
+    double nu;           /* nu (LBM.h:65-66)                                   */
+    double magic_f;      /* V, fluid TRT magic parameter (LBM.h:110)           */
+    double diff_p;       /* diffu, c+ diffusivity (LBM.h:64)                   */
+    double magic_p;      /* VC (LBM.h:111)                                     */
+    double mob_p;        /* K, c+ mobility (LBM.h:67-68)                       */
+    double diff_n;       /* D, c- diffusivity (LBM.h:71-72)                    */
+    double magic_n;      /* VT (LBM.h:112)                                     */
+    double mob_n;        /* Kn, c- mobility (LBM.h:74-75)                      */
+    double eps;          /* eps, permittivity (LBM.h:63)                       */
+    double f_charge;     /* convertCtoCharge (LBM.h:90)                        */
+    double zeta_lo;      /* voltage, wall potential at y = 0 (LBM.h:58)        */
+    double zeta_hi;      /* voltage2, wall potential at y = ny-1 (LBM.h:60)    */
+    double cp_lo, cp_hi; /* charge0, charge1: c+ at the walls (LBM.h:55-56)    */
+    double cn_lo, cn_hi; /* charge0n, charge1n: c- at the walls (LBM.h:81-83)  */
+    double ext_x;        /* Ext, applied field along x (LBM.h:62)              */
+    double exf;          /* exf, extra body force along x (LBM.h:47-49)        */
+    double uw;           /* uw, top wall velocity (LBM.h:46-48)                */
+} ek_params;
+
+typedef struct ek_ctx ek_ctx;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int ek_version(void);
+const char *ek_status_string(int status);
+/* Message of the last failing call on this host thread ("" if none). */
+const char *ek_last_error(void);
+
+/* Fill *p with lattice-unit defaults (dx=dy=dt=cfl=1, cs2=1/3, nu=1/6,
+ * magic 1/4, FP64 storage, force and rest quirk on).  nx, ny are set. */
+int ek_params_default(ek_params *p, int32_t nx, int32_t ny);
+
+/* Make `device` the current CUDA device of this library on the calling host
+ * thread (the library carries its own CUDA runtime state, so a device chosen
+ * through another runtime instance, e.g. a Python framework's, does not apply). */
+int ek_set_device(int32_t device);
+int ek_get_device_count(int32_t *out);
+
+/* Create a context on the current CUDA device.  Replaces the allocation and
+ * set-up block of main.cu:89-142 (population and field buffers, cuFFT plan,
+ * wavenumber tables).  Rejects invalid parameters with EK_ERR_INVALID. */
+int ek_create(const ek_params *p, ek_ctx **out);
+int ek_destroy(ek_ctx *ctx);
+/* Run all later work of ctx on this stream (a cudaStream_t; NULL = legacy). */
+int ek_set_stream(ek_ctx *ctx, void *stream);
+int ek_get_params(const ek_ctx *ctx, ek_params *out);
+
+/* Load macroscopic fields (host pointers, nx*ny doubles each).  ex/ey may be
+ * NULL: the field is then taken from psi.  Mirrors read_data (LBM.cu:1350-1391)
+ * minus the file parsing. */
+int ek_set_fields(ek_ctx *ctx, const double *rho, const double *ux,
+                  const double *uy, const double *cp, const double *cn,
+                  const double *psi, const double *ex, const double *ey);
+
+/* Per-x wall potential and wall concentrations (nx doubles each, any may be
+ * NULL to keep the uniform value).  Extends the uniform voltage/charge0
+ * constants of LBM.h:55-83 to a wall zeta that varies along x. */
+int ek_set_wall_profile(ek_ctx *ctx, const double *zeta_lo, const double *zeta_hi,
+                        const double *cp_lo, const double *cp_hi,
+                        const double *cn_lo, const double *cn_hi);
+
+/* Populations at equilibrium with the loaded fields: init_equilibrium /
+ * gpu_init_equilibrium (LBM.cu:183-305). */
+int ek_init_equilibrium(ek_ctx *ctx);
+
+/* Advance nsteps coupled steps.  One step = stream_collide_save
+ * (LBM.cu:307-329: collide, fluid walls, stream, ion walls) followed by
+ * fast_Poisson (poisson.cu:180-208), fused as one pull-scheme LBM kernel plus
+ * a three-pass Poisson solve. */
+int ek_step(ek_ctx *ctx, int32_t nsteps);
+
+/* Poisson solve for the current c+, c- moments, then psi and E:
+ * fast_Poisson (poisson.cu:180-208) without its per-call cudaMalloc/Free. */
+int ek_poisson(ek_ctx *ctx);
+
+/* Copy the macroscopic fields of the last step to host arrays (any pointer may
+ * be NULL).  rho, ux, uy, cp, cn are the moments of the last step's
+ * pre-collision populations, psi/ex/ey the Poisson result from them, as the
+ * reference's buffers hold after its loop (main.cu:190-233). */
+int ek_get_fields(ek_ctx *ctx, double *rho, double *ux, double *uy, double *cp,
+                  double *cn, double *psi, double *ex, double *ey);
+
+/* Same as ek_get_fields but into device buffers of nx*ny doubles. */
+int ek_get_fields_device(ek_ctx *ctx, double *rho, double *ux, double *uy,
+                         double *cp, double *cn, double *psi, double *ex,
+                         double *ey);
+
+/* Steady-state residual over the last `interval` steps (new; the reference has
+ * none): out[q] = ||q^n - q^{n-interval}||_2 / (interval * max(||q^n||_2, floor_q))
+ * for q = ux, c+, c-, psi (FP64 reductions on the device); out[4] = max.
+ * Returns EK_ERR_NAN if a field holds a non-finite value.  The first call only
+ * records the snapshot and reports out[] = +inf. */
+int ek_residual(ek_ctx *ctx, int32_t interval, double *out5);
+
+/* Steps taken since ek_create / ek_init_equilibrium. */
+int ek_step_count(const ek_ctx *ctx, int64_t *out);
+
+/* Wait for the context's stream. */
+int ek_sync(ek_ctx *ctx);
+
+/* Device pointers of the field planes (zero-copy readers).  Order: rho, ux,
+ * uy, cp, cn, psi, ex, ey; each plane has ny rows of *pitch doubles (pitch >=
+ * nx), index = pitch*y + x. */
+int ek_field_pointers(ek_ctx *ctx, double **out8, int32_t *pitch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EKPNP_H */

@@ -1,0 +1,151 @@
+"""Build the patched reference (gyf135/EK-PNP) for the parity cases.  TEST
+INFRASTRUCTURE: its binaries are the pin for the CPU oracle and the FP64 GPU
+path; nothing in the product runs them.
+
+Recipe, per case in oracle/cases.py:
+  1. copy main.cu, LBM.cu, LBM.h, poisson.cu, seconds.cpp, seconds.h from the
+     reference checkout (default /root/reference, read-only) to a temporary
+     directory -- the sources never enter this repository;
+  2. patch the copy:
+       LBM.h    compile-time sizes, NSTEPS, restart flag = 1 (read_data path,
+                main.cu:165-171), nThreads dividing NX, and the physics
+                constants in lattice units (see oracle/cases.py);
+       LBM.cu   enable the electric body force exactly as written in the
+                comments at LBM.cu:388-389 and 438-439 (cases with force on);
+       main.cu  dump rho, ux, uy, c+, c-, phi, Ex, Ey as raw doubles with the
+                reference's own save_scalar (LBM.cu:1062) after the loop;
+  3. nvcc -O3 -gencode arch=compute_100a,code=sm_100a main.cu seconds.cpp -lcufft
+     into oracle/_ref/<case>/ekref (git-ignored; it travels to the GPU box with
+     the working tree).
+
+The loop in main.cu runs NSTEPS+1 steps (main.cu:190), so NSTEPS = steps-1.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+import re
+import shutil
+import subprocess
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+from cases import CASES, FLAG_FORCE, FLAG_REST_QUIRK  # noqa: E402
+
+REF_DIR = os.environ.get("EKPNP_REFERENCE", "/root/reference")
+OUT_DIR = os.path.join(HERE, "_ref")
+SOURCES = ("main.cu", "LBM.cu", "LBM.h", "poisson.cu", "seconds.cpp", "seconds.h")
+NVCC = os.environ.get("NVCC", "nvcc")
+
+
+def _lit(v: float) -> str:
+    r = repr(float(v))
+    return r if ("e" in r or "." in r or "n" in r) else r + ".0"
+
+
+def _sub1(text: str, pattern: str, repl: str, what: str, count: int = 1) -> str:
+    new, n = re.subn(pattern, repl, text)
+    if n != count:
+        raise RuntimeError(f"reference patch '{what}' matched {n} times, expected {count}")
+    return new
+
+
+def _threads_for(nx: int) -> int:
+    for t in (128, 64, 32, 16, 10, 8, 5, 4, 2, 1):
+        if nx % t == 0:
+            return t
+    return 1
+
+
+def patch_sources(src: dict, p: dict, steps: int) -> dict:
+    if p["flags"] & FLAG_REST_QUIRK == 0:
+        raise RuntimeError("the reference build always has the rest-equilibrium quirk")
+    h = src["LBM.h"]
+    ints = {
+        r"const unsigned int flag": 1,
+        r"const int nThreads": _threads_for(p["nx"]),
+        r"const unsigned int NX": p["nx"],
+        r"const unsigned int NY": p["ny"],
+        r"const unsigned int NSTEPS": steps - 1,
+        r"const unsigned int NSAVE": 1000000000,
+    }
+    for decl, v in ints.items():
+        h = _sub1(h, decl + r"\s*=\s*[^;]+;", f"{decl.replace(chr(92), '')} = {v};", decl)
+    consts = {
+        "LL": p["lx"], "Lx": p["lx"], "Ly": (p["ny"] - 1) * p["dy"], "dx": p["dx"],
+        "dy": p["dy"], "CFL": p["cfl"], "dt": p["dt"], "cs_square": p["cs2"],
+        "rho0": p["rho0"], "chargeinf": p["c0"], "charge0": p["cp_lo"], "charge1": p["cp_hi"],
+        "voltage": p["zeta_lo"], "voltage2": p["zeta_hi"], "Ext": p["ext_x"], "eps": p["eps"],
+        "diffu": p["diff_p"], "charge0n": p["cn_lo"], "charge1n": p["cn_hi"],
+        "convertCtoCharge": p["f_charge"], "V": p["magic_f"], "VC": p["magic_p"],
+        "VT": p["magic_n"],
+    }
+    for name, v in consts.items():
+        h = _sub1(h, r"(__constant__ double\s+" + name + r"\s*=\s*)[^;]+;",
+                  r"\g<1>" + _lit(v) + ";", name)
+    hosts = {"nu_host": p["nu"], "K_host": p["mob_p"], "D_host": p["diff_n"],
+             "Kn_host": p["mob_n"], "uw_host": p["uw"], "exf_host": p["exf"]}
+    for name, v in hosts.items():
+        h = _sub1(h, r"(\ndouble\s+" + name + r"\s*=\s*)[^;]+;", r"\g<1>" + _lit(v) + ";", name)
+    src["LBM.h"] = h
+
+    if p["flags"] & FLAG_FORCE:
+        src["LBM.cu"] = _sub1(src["LBM.cu"], r"double (force[xy]m?) = 0;//\s*([^;\n]+);",
+                              r"double \1 = \2;", "electric body force", count=4)
+
+    dumps = "".join(
+        f'\tsave_scalar("{n}", {g}, scalar_host, 0);\n'
+        for n, g in (("rho", "rho_gpu"), ("ux", "ux_gpu"), ("uy", "uy_gpu"),
+                     ("cp", "charge_gpu"), ("cn", "T_gpu"), ("psi", "phi_gpu"),
+                     ("ex", "Ex_gpu"), ("ey", "Ey_gpu")))
+    src["main.cu"] = _sub1(src["main.cu"], r"(\n\s*// destory event objects)",
+                           "\n" + dumps.replace("\\", "\\\\") + r"\1", "dump block")
+    return src
+
+
+def build_case(name: str, force: bool = False) -> str:
+    p, seed, steps = CASES[name]
+    out = os.path.join(OUT_DIR, name)
+    exe = os.path.join(out, "ekref")
+    meta = os.path.join(out, "case.json")
+    want = dict(params=p, seed=seed, steps=steps)
+    if not force and os.path.exists(exe) and os.path.exists(meta):
+        with open(meta) as fh:
+            if json.load(fh) == json.loads(json.dumps(want)):
+                return exe
+    if not os.path.isdir(REF_DIR):
+        raise FileNotFoundError(f"reference checkout not found at {REF_DIR}")
+    src = {}
+    for f in SOURCES:
+        with open(os.path.join(REF_DIR, f), encoding="latin-1") as fh:
+            src[f] = fh.read()
+    src = patch_sources(src, p, steps)
+    os.makedirs(out, exist_ok=True)
+    with tempfile.TemporaryDirectory(prefix="ekref_") as tmp:
+        for f, text in src.items():
+            with open(os.path.join(tmp, f), "w", encoding="latin-1") as fh:
+                fh.write(text)
+        cmd = [NVCC, "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-w",
+               "main.cu", "seconds.cpp", "-lcufft", "-o", exe]
+        r = subprocess.run(cmd, cwd=tmp, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("reference build failed:\n" + r.stdout + r.stderr)
+    with open(meta, "w") as fh:
+        json.dump(want, fh, indent=1)
+    return exe
+
+
+def build_all(names=None) -> list:
+    return [build_case(n) for n in (names or CASES)]
+
+
+def available() -> bool:
+    return os.path.isdir(REF_DIR) and shutil.which(NVCC) is not None
+
+
+if __name__ == "__main__":
+    for path in build_all(sys.argv[1:] or None):
+        print(path)
