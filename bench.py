@@ -1,0 +1,320 @@
+"""Benchmark of the coupled EK-PNP step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload channel-4096x1024] [--storage f32|f16|f64]
+
+One step = one coupled update of one channel: the fused LBM kernel (fluid +
+two ion species, walls, streaming, Guo force) and the Poisson solve (row FFTs,
+tridiagonal column solves, inverse row FFTs).  Metric: coupled MLUPS =
+nx*ny*steps / seconds, summed over ranks.  N > 1 runs one independent channel
+per GPU (replicas; the single-channel path does not shard), so scaling is weak.
+
+The device-timed region holds exactly K steps between CUDA events on the
+solver's stream, after W warm-up steps, with a barrier and a stream
+synchronisation on both sides; the working set (two population buffers of
+27 planes) is several times the 126 MB L2, so no flush is needed.  `e2e` runs
+the same K steps through the public API from pinned host buffers: fields in
+(H2D), equilibrium initialisation, steps in chunks of 100 with a residual
+read-back after each, fields out (D2H), timed by the host clock.
+
+--impl reference times the CPU oracle (the OpenMP restatement of the
+reference's update rules; the reference itself has no CPU path) on the same
+workload, on rank 0 only, for a bounded number of full steps.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "ek-pnp_b200"))
+
+STORAGE = {"f64": 0, "f32": 1, "f16": 2}
+POP_BYTES = {"f64": 8, "f32": 4, "f16": 2}
+CPU_SAMPLE_S = 15.0
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def measured_peak_gbs():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(workload, storage):
+    """DRAM bytes per launch of the LBM kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", f"lbm_{storage}_{workload}.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["dram_bytes_per_launch"])
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, local_rank):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        self.index = vis.split(",")[local_rank] if vis else str(local_rank)
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.index, f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in out.strip().splitlines():
+            f = [v.strip() for v in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+class Dist:
+    def __init__(self, use_pg=True):
+        self.world = env_int("WORLD_SIZE", 1)
+        self.rank = env_int("RANK", 0)
+        self.local = env_int("LOCAL_RANK", 0)
+        self.pg = None
+        if self.world > 1 and use_pg:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", self.local))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v):
+        if not self.pg:
+            return v
+        import torch
+        t = torch.tensor([float(v)], device=f"cuda:{self.local}", dtype=torch.float64)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.barrier()
+            self.pg.destroy_process_group()
+
+
+def cpu_oracle_rate(params, seed, max_steps, budget_s):
+    """Coupled MLUPS of the CPU oracle with all host threads, full steps of the
+    same channel until budget_s elapsed (at least one step)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from ekpnp import noisy_uniform_state
+    oracle.build()
+    threads = oracle.set_threads(0)
+    p = dict(params, storage=0)
+    o = oracle.OracleChannel(p)
+    o.set_fields(**noisy_uniform_state(p["nx"], p["ny"], seed))
+    o.init_equilibrium()
+    o.step(1)  # warm-up: page in, build FFT plans
+    steps, t0 = 0, time.perf_counter()
+    while steps < max_steps:
+        o.step(1)
+        steps += 1
+        if time.perf_counter() - t0 >= budget_s:
+            break
+    dt = time.perf_counter() - t0
+    o.close()
+    return p["nx"] * p["ny"] * steps / dt / 1e6, threads, steps, dt
+
+
+def run_reference(args, d):
+    from ekpnp import workload_params, WORKLOADS
+    if d.rank != 0:
+        return 0
+    p = workload_params(args.workload)
+    w = WORKLOADS[args.workload]
+    budget = min(120.0, max(10.0, 0.05 * args.steps))
+    rate, threads, steps, dt = cpu_oracle_rate(p, w["seed"], args.steps, budget)
+    sample = f"{steps} full coupled FP64 steps of the {w['nx']}x{w['ny']} channel in {dt:.1f} s"
+    line = {
+        "metric": "coupled_mlups", "value": rate, "unit": "MLUPS", "impl": "reference",
+        "n_gpus": args.gpus, "steps": steps, "warmup": 1, "ms_per_step": dt / steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded noisy uniform state)",
+        "config": {"workload": args.workload, "nx": w["nx"], "ny": w["ny"], "storage": "f64",
+                   "host_threads": threads},
+        "cpu_baseline": {"value": rate, "unit": "MLUPS", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": rate, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, d):
+    import torch
+    import ekpnp
+    from ekpnp import Channel, WORKLOADS, noisy_uniform_state, workload_params
+    w = WORKLOADS[args.workload]
+    nx, ny, nn = w["nx"], w["ny"], w["nx"] * w["ny"]
+    ekpnp.set_device(d.local)
+    p = workload_params(args.workload, storage=STORAGE[args.storage])
+    init = noisy_uniform_state(nx, ny, w["seed"] + d.rank)
+
+    # ---- device-timed region ----
+    ch = Channel(p)
+    ch.set_fields(**init)
+    ch.init_equilibrium()
+    ch.step(args.warmup)
+    ch.sync()
+    clocks = ClockSampler(d.local)
+    clocks.start()
+    time.sleep(0.3)
+    d.barrier()
+    ch.sync()
+    n_launch0 = ch.launches
+    ch.profile(True)
+    ch.mark(0)
+    ch.step(args.steps)
+    ch.mark(1)
+    ms = ch.elapsed_ms(0, 1)
+    ch.sync()
+    d.barrier()
+    launches = ch.launches - n_launch0
+    prof = ch.profile_read()
+    ch.profile(False)
+    clk = clocks.stop()
+    ms_max = d.max(ms)
+    value = d.world * nn * args.steps / (ms_max / 1e3) / 1e6
+
+    # ---- roofline of the dominant kernel (the fused LBM step) ----
+    lbm_ms, lbm_n = prof["lbm"]
+    per_launch_s = lbm_ms / max(lbm_n, 1) / 1e3
+    bytes_node = 54 * POP_BYTES[args.storage] + 16  # 27 pops in + 27 out, psi in, rhs out (FP64)
+    achieved = nn * bytes_node / per_launch_s / 1e9
+    peak, peak_kind = measured_peak_gbs()
+    traffic = ncu_traffic(args.workload, args.storage)
+    step_ms = ms / args.steps
+    shares = {k: round(v[0] / max(sum(x[0] for x in prof.values()), 1e-12), 4) for k, v in prof.items()}
+    ch.close()
+
+    # ---- end to end through the public API, pinned host buffers ----
+    pin = {k: torch.from_numpy(init[k]).pin_memory() for k in ("rho", "ux", "uy", "cp", "cn", "psi")}
+    outs = {k: torch.empty((ny, nx), dtype=torch.float64).pin_memory() for k in ("ux", "cp", "cn", "psi")}
+    order = ("rho", "ux", "uy", "cp", "cn", "psi", "ex", "ey")
+    chunk = 100
+    reps = max(1, args.steps // chunk)
+    ch = Channel(p)
+    ch.set_fields(**init)
+    ch.init_equilibrium()
+    ch.step(min(args.warmup, 10))
+    ch.sync()
+    d.barrier()
+    t0 = time.perf_counter()
+    ch.set_fields_from_pointers([pin[k].data_ptr() if k in pin else 0 for k in order])
+    ch.init_equilibrium()
+    for _ in range(reps):
+        ch.step(chunk)
+        ch.residual(chunk)
+    ch.get_fields_to_pointers([outs[k].data_ptr() if k in outs else 0 for k in order])
+    e2e_s = d.max(time.perf_counter() - t0)
+    ch.close()
+    e2e_steps = reps * chunk
+    e2e = {"value": d.world * nn * e2e_steps / e2e_s / 1e6, "unit": "MLUPS",
+           "h2d_bytes_per_step": 6 * nn * 8 / e2e_steps,
+           "d2h_bytes_per_step": (4 * nn * 8 + reps * 5 * 8) / e2e_steps,
+           "steps": e2e_steps}
+
+    cpu = None
+    if d.world == 1 and d.rank == 0 and not args.no_cpu_baseline:
+        rate, threads, steps, dt = cpu_oracle_rate(workload_params(args.workload), w["seed"], 10 ** 6, CPU_SAMPLE_S)
+        cpu = {"value": rate, "unit": "MLUPS", "cores": threads, "kind": "port",
+               "sample": f"{steps} full coupled FP64 steps of the {nx}x{ny} channel in {dt:.1f} s"}
+
+    if d.rank == 0:
+        line = {
+            "metric": "coupled_mlups", "value": value, "unit": "MLUPS", "n_gpus": d.world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": {"f64": "f64", "f32": "f32", "f16": "f32 (f16 storage)"}[args.storage],
+            "data": "synthetic (seeded noisy uniform state, u = psi = 0)",
+            "config": {"workload": args.workload, "nx": nx, "ny": ny, "storage": args.storage + "-shifted"
+                       if args.storage != "f64" else "f64", "kappa_h": w["kappa_h"], "zeta": w["zeta"],
+                       "e_x": w["ex"], "parallelism": f"replicas x{d.world}",
+                       "l2": "working set > 126 MB L2 (2 x 27 population planes), no flush"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "fused LBM step", "bytes_per_node": bytes_node,
+                         "launch_ms": per_launch_s * 1e3},
+            "step_breakdown": {"ms_per_step": step_ms, "share": shares},
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", default="channel-4096x1024")
+    ap.add_argument("--storage", choices=tuple(STORAGE), default="f32")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    d = Dist(use_pg=args.impl == "ours")
+    try:
+        rc = run_reference(args, d) if args.impl == "reference" else run_ours(args, d)
+    finally:
+        d.close()
+    return rc
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -48,7 +48,7 @@ struct ek_ctx {
     bool own_stream = false;
     int nxp = 0, mp = 0, n = 0;
     size_t plane = 0;
-    double *pops[2] = {nullptr, nullptr};
+    void *pops[2] = {nullptr, nullptr};
     int cur = 0;
     bool initialised = false;  // populations exist
     bool state_pre = false;    // pops[cur] holds pre-collision populations in place
@@ -64,6 +64,13 @@ struct ek_ctx {
     PoissonPlan pp{};
     Chan chan{};
     int64_t steps = 0;
+    int64_t launches = 0;
+    // profiling
+    bool prof = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
+    std::vector<int> ev_phase;
+    size_t ev_used = 0;
+    cudaEvent_t marks[16] = {};
 };
 
 namespace {
@@ -73,7 +80,6 @@ int validate(const ek_params *p) {
     if (p->nx < 2 || p->ny < 4) return fail(EK_ERR_INVALID, "need nx >= 2 and ny >= 4");
     if (p->storage != EK_STORE_F64 && p->storage != EK_STORE_F32 && p->storage != EK_STORE_F16)
         return fail(EK_ERR_INVALID, "unknown storage mode");
-    if (p->storage != EK_STORE_F64) return fail(EK_ERR_UNSUPPORTED, "storage mode not built yet");
     if (is_pow2(p->nx) ? p->nx > 8192 : p->nx > 2048)
         return fail(EK_ERR_UNSUPPORTED, "nx above 8192 (powers of two) or 2048 (other lengths)");
     if (p->ny > 65535) return fail(EK_ERR_UNSUPPORTED, "ny above 65535");
@@ -103,6 +109,12 @@ void free_ctx(ek_ctx *c) {
     cudaFree(c->pp.tw);
     cudaFree(c->pp.piv);
     cudaFree(c->pp.spec);
+    for (auto &pr : c->ev_pool) {
+        cudaEventDestroy(pr.first);
+        cudaEventDestroy(pr.second);
+    }
+    for (auto &m : c->marks)
+        if (m) cudaEventDestroy(m);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -183,15 +195,46 @@ int copy_out(ek_ctx *c, int plane_idx, double *dst, cudaMemcpyKind kind) {
 int refresh_e(ek_ctx *c) {
     if (c->e_stale && !(c->p.flags & EK_FLAG_EXPLICIT_E)) {
         EK_CUDA(launch_efield_f64(c->chan, c->fields, c->stream), "efield kernel");
+        ++c->launches;
         c->e_stale = false;
     }
     return EK_OK;
 }
 
+// Launch one kernel of `phase` through fn(); with profiling on, bracket it
+// with a pair of events from the context's pool.
+template <typename Fn>
+int timed(ek_ctx *c, int phase, const char *what, Fn fn) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (c->prof) {
+        if (c->ev_used == c->ev_pool.size()) {
+            cudaEvent_t e0, e1;
+            EK_CUDA(cudaEventCreate(&e0), "event create");
+            EK_CUDA(cudaEventCreate(&e1), "event create");
+            c->ev_pool.emplace_back(e0, e1);
+            c->ev_phase.push_back(0);
+        }
+        a = c->ev_pool[c->ev_used].first;
+        b = c->ev_pool[c->ev_used].second;
+        c->ev_phase[c->ev_used] = phase;
+        ++c->ev_used;
+        EK_CUDA(cudaEventRecord(a, c->stream), "event record");
+    }
+    EK_CUDA(fn(), what);
+    ++c->launches;
+    if (c->prof) EK_CUDA(cudaEventRecord(b, c->stream), "event record");
+    return EK_OK;
+}
+
 int poisson_now(ek_ctx *c) {
-    EK_CUDA(poisson_solve_f64(c->pp, c->chan, c->fields, c->stream), "poisson kernels");
+    for (int pass = 0; pass < 3; ++pass) {
+        int rc = timed(c, 1 + pass, "poisson kernel",
+                       [&] { return poisson_pass_f64(pass, c->pp, c->chan, c->fields, c->stream); });
+        if (rc != EK_OK) return rc;
+    }
     if (c->p.flags & EK_FLAG_EXPLICIT_E) {
         EK_CUDA(launch_efield_f64(c->chan, c->fields, c->stream), "efield kernel");
+        ++c->launches;
     } else {
         c->e_stale = true;
     }
@@ -282,7 +325,7 @@ int ek_create(const ek_params *p, ek_ctx **out) {
     c->plane = (size_t)p->ny * c->nxp;
     c->n = p->ny - 2;
     c->mp = round_up(p->nx / 2 + 1, 16);
-    const size_t pop_bytes = 27 * c->plane * sizeof(double);
+    const size_t pop_bytes = 27 * c->plane * pop_elem_bytes(p->storage);
     struct Alloc { void **ptr; size_t bytes; } allocs[] = {
         {(void **)&c->pops[0], pop_bytes},
         {(void **)&c->pops[1], pop_bytes},
@@ -387,7 +430,10 @@ int ek_set_wall_profile(ek_ctx *c, const double *zlo, const double *zhi, const d
 int ek_init_equilibrium(ek_ctx *c) {
     if (!c) return fail(EK_ERR_INVALID, "null context");
     const bool ee = c->explicit_e_once || (c->p.flags & EK_FLAG_EXPLICIT_E);
-    EK_CUDA(launch_init_f64(c->chan, c->pops[c->cur], c->fields, ee, c->stream), "init kernel");
+    if (c->p.storage == EK_STORE_F64)
+        EK_CUDA(launch_init_f64(c->chan, (double *)c->pops[c->cur], c->fields, ee, c->stream), "init kernel");
+    else
+        EK_CUDA(launch_init_shifted(c->chan, c->p.storage, c->pops[c->cur], c->fields, ee, c->stream), "init kernel");
     c->initialised = true;
     c->state_pre = true;
     c->steps = 0;
@@ -401,9 +447,15 @@ int ek_step(ek_ctx *c, int32_t nsteps) {
     const bool every = (c->p.flags & EK_FLAG_MOMENTS_EVERY_STEP) != 0;
     for (int32_t i = 0; i < nsteps; ++i) {
         const bool ee = c->explicit_e_once || (c->p.flags & EK_FLAG_EXPLICIT_E);
-        EK_CUDA(launch_step_f64(c->chan, c->pops[c->cur], c->pops[c->cur ^ 1], c->fields, c->state_pre, ee,
-                                every || i == nsteps - 1, c->stream),
-                "LBM step kernel");
+        const bool mom = every || i == nsteps - 1;
+        int rc0 = timed(c, 0, "LBM step kernel", [&] {
+            if (c->p.storage == EK_STORE_F64)
+                return launch_step_f64(c->chan, (const double *)c->pops[c->cur], (double *)c->pops[c->cur ^ 1],
+                                       c->fields, c->state_pre, ee, mom, c->stream);
+            return launch_step_shifted(c->chan, c->p.storage, c->pops[c->cur], c->pops[c->cur ^ 1], c->fields,
+                                       c->state_pre, ee, mom, c->stream);
+        });
+        if (rc0 != EK_OK) return rc0;
         c->cur ^= 1;
         c->state_pre = false;
         c->explicit_e_once = false;
@@ -493,6 +545,56 @@ int ek_step_count(const ek_ctx *c, int64_t *out) {
 int ek_sync(ek_ctx *c) {
     if (!c) return fail(EK_ERR_INVALID, "null context");
     EK_CUDA(cudaStreamSynchronize(c->stream), "sync");
+    return EK_OK;
+}
+
+int ek_profile_enable(ek_ctx *c, int32_t on) {
+    if (!c) return fail(EK_ERR_INVALID, "null context");
+    EK_CUDA(cudaStreamSynchronize(c->stream), "profile sync");
+    c->prof = on != 0;
+    c->ev_used = 0;
+    return EK_OK;
+}
+
+int ek_profile_read(ek_ctx *c, double *ms4, int64_t *launches4) {
+    if (!c || !ms4 || !launches4) return fail(EK_ERR_INVALID, "null argument");
+    EK_CUDA(cudaStreamSynchronize(c->stream), "profile sync");
+    for (int k = 0; k < 4; ++k) {
+        ms4[k] = 0.0;
+        launches4[k] = 0;
+    }
+    for (size_t i = 0; i < c->ev_used; ++i) {
+        float ms = 0.0f;
+        EK_CUDA(cudaEventElapsedTime(&ms, c->ev_pool[i].first, c->ev_pool[i].second), "event elapsed");
+        const int ph = c->ev_phase[i];
+        if (ph >= 0 && ph < 4) {
+            ms4[ph] += ms;
+            ++launches4[ph];
+        }
+    }
+    return EK_OK;
+}
+
+int ek_mark(ek_ctx *c, int32_t slot) {
+    if (!c || slot < 0 || slot >= 16) return fail(EK_ERR_INVALID, "bad event slot");
+    if (!c->marks[slot]) EK_CUDA(cudaEventCreate(&c->marks[slot]), "event create");
+    EK_CUDA(cudaEventRecord(c->marks[slot], c->stream), "event record");
+    return EK_OK;
+}
+
+int ek_elapsed(ek_ctx *c, int32_t a, int32_t b, double *ms) {
+    if (!c || !ms || a < 0 || a >= 16 || b < 0 || b >= 16 || !c->marks[a] || !c->marks[b])
+        return fail(EK_ERR_INVALID, "bad event slots");
+    EK_CUDA(cudaEventSynchronize(c->marks[b]), "event sync");
+    float f = 0.0f;
+    EK_CUDA(cudaEventElapsedTime(&f, c->marks[a], c->marks[b]), "event elapsed");
+    *ms = f;
+    return EK_OK;
+}
+
+int ek_launch_count(const ek_ctx *c, int64_t *out) {
+    if (!c || !out) return fail(EK_ERR_INVALID, "null argument");
+    *out = c->launches;
     return EK_OK;
 }
 

@@ -64,6 +64,13 @@ cudaError_t launch_step_f64(const Chan &c, const double *src, double *dst, doubl
 cudaError_t launch_efield_f64(const Chan &c, double *fields, cudaStream_t s);
 cudaError_t launch_rhs_from_moments_f64(const Chan &c, double *fields, cudaStream_t s);
 
+// ---- shifted-storage forms (ek_lbm_f32.cu); storage = EK_STORE_F32 or _F16 ----
+cudaError_t launch_step_shifted(const Chan &c, int storage, const void *src, void *dst, double *fields,
+                                bool first, bool explicit_e, bool moments, cudaStream_t s);
+cudaError_t launch_init_shifted(const Chan &c, int storage, void *pops, const double *fields, bool explicit_e,
+                                cudaStream_t s);
+inline size_t pop_elem_bytes(int storage) { return storage == EK_STORE_F64 ? 8 : (storage == EK_STORE_F32 ? 4 : 2); }
+
 // ---- Poisson (ek_poisson.cu) ----
 struct PoissonPlan {
     int nx, ny, n, mp, log2nx;  // n = ny-2 interior rows
@@ -73,7 +80,8 @@ struct PoissonPlan {
     double *piv;                // n x mp pivots
     double2 *spec;              // n x mp spectrum
 };
-cudaError_t poisson_solve_f64(const PoissonPlan &pp, const Chan &c, double *fields, cudaStream_t s);
+// pass 0: row FFTs, 1: tridiagonal column solve, 2: inverse row FFTs + walls
+cudaError_t poisson_pass_f64(int pass, const PoissonPlan &pp, const Chan &c, double *fields, cudaStream_t s);
 size_t poisson_smem_bytes_f64(int nx);
 cudaError_t poisson_set_smem_limits();
 

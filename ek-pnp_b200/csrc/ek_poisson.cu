@@ -176,12 +176,12 @@ size_t poisson_smem_bytes_f64(int nx) {
     return (size_t)nx * sizeof(double2) * (pow2 ? 1 : 2);
 }
 
-cudaError_t poisson_solve_f64(const PoissonPlan &pp, const Chan &c, double *fields, cudaStream_t s) {
+cudaError_t poisson_pass_f64(int pass, const PoissonPlan &pp, const Chan &c, double *fields, cudaStream_t s) {
     const size_t smem = poisson_smem_bytes_f64(pp.nx);
     const int rows2 = (pp.n + 1) / 2;
-    fwd_rows<<<rows2, PTPB, smem, s>>>(pp, fields + F_RHS * c.plane, c.nxp);
-    tridiag<<<(pp.nx / 2 + 1 + PTPB - 1) / PTPB, PTPB, 0, s>>>(pp);
-    inv_rows<<<rows2, PTPB, smem, s>>>(pp, c, fields + F_PSI * c.plane);
+    if (pass == 0) fwd_rows<<<rows2, PTPB, smem, s>>>(pp, fields + F_RHS * c.plane, c.nxp);
+    else if (pass == 1) tridiag<<<(pp.nx / 2 + 1 + PTPB - 1) / PTPB, PTPB, 0, s>>>(pp);
+    else inv_rows<<<rows2, PTPB, smem, s>>>(pp, c, fields + F_PSI * c.plane);
     return cudaGetLastError();
 }
 

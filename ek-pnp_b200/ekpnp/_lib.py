@@ -77,6 +77,11 @@ _SIGS = {
     "ek_step_count": ([ctypes.c_void_p, _P(ctypes.c_int64)], ctypes.c_int),
     "ek_sync": ([ctypes.c_void_p], ctypes.c_int),
     "ek_field_pointers": ([ctypes.c_void_p, _P(ctypes.c_void_p), _P(ctypes.c_int32)], ctypes.c_int),
+    "ek_profile_enable": ([ctypes.c_void_p, ctypes.c_int32], ctypes.c_int),
+    "ek_profile_read": ([ctypes.c_void_p, _dp, _P(ctypes.c_int64)], ctypes.c_int),
+    "ek_mark": ([ctypes.c_void_p, ctypes.c_int32], ctypes.c_int),
+    "ek_elapsed": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, _dp], ctypes.c_int),
+    "ek_launch_count": ([ctypes.c_void_p, _P(ctypes.c_int64)], ctypes.c_int),
 }
 
 

@@ -116,5 +116,43 @@ class Channel:
         check(lib().ek_step_count(self._h, ctypes.byref(v)))
         return int(v.value)
 
+    # -- profiling ----------------------------------------------------------
+    PHASES = ("lbm", "poisson_rows_fwd", "poisson_tridiag", "poisson_rows_inv")
+
+    def profile(self, on=True):
+        check(lib().ek_profile_enable(self._h, 1 if on else 0))
+
+    def profile_read(self):
+        ms = (ctypes.c_double * 4)()
+        n = (ctypes.c_int64 * 4)()
+        check(lib().ek_profile_read(self._h, ms, n))
+        return {ph: (float(ms[i]), int(n[i])) for i, ph in enumerate(self.PHASES)}
+
+    def mark(self, slot):
+        check(lib().ek_mark(self._h, int(slot)))
+
+    def elapsed_ms(self, a, b):
+        v = ctypes.c_double()
+        check(lib().ek_elapsed(self._h, int(a), int(b), ctypes.byref(v)))
+        return float(v.value)
+
+    @property
+    def launches(self):
+        v = ctypes.c_int64()
+        check(lib().ek_launch_count(self._h, ctypes.byref(v)))
+        return int(v.value)
+
+    def set_fields_from_pointers(self, ptrs):
+        """set_fields from raw host addresses (e.g. pinned buffers); ptrs is a
+        sequence of 8 integers (0 = leave the field unchanged)."""
+        dp = ctypes.POINTER(ctypes.c_double)
+        args = [ctypes.cast(ctypes.c_void_p(p), dp) if p else None for p in ptrs]
+        check(lib().ek_set_fields(self._h, *args))
+
+    def get_fields_to_pointers(self, ptrs):
+        dp = ctypes.POINTER(ctypes.c_double)
+        args = [ctypes.cast(ctypes.c_void_p(p), dp) if p else None for p in ptrs]
+        check(lib().ek_get_fields(self._h, *args))
+
     def set_stream(self, stream_handle: int):
         check(lib().ek_set_stream(self._h, ctypes.c_void_p(stream_handle)))

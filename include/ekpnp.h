@@ -185,6 +185,21 @@ int ek_sync(ek_ctx *ctx);
  * nx), index = pitch*y + x. */
 int ek_field_pointers(ek_ctx *ctx, double **out8, int32_t *pitch);
 
+/* ---- profiling (CUDA events on the context's stream) ------------------
+ * Phases of a step: 0 = fused LBM kernel, 1 = Poisson pass A (row FFTs),
+ * 2 = pass B (tridiagonal y-solve), 3 = pass C (inverse row FFTs).
+ * ek_profile_enable(ctx, 1) resets and starts per-launch timing;
+ * ek_profile_read waits for the stream and returns, per phase, the summed
+ * kernel milliseconds and the launch count since the last enable. */
+int ek_profile_enable(ek_ctx *ctx, int32_t on);
+int ek_profile_read(ek_ctx *ctx, double *ms4, int64_t *launches4);
+/* Record event `slot` (0..15) on the context's stream; elapsed ms between two
+ * recorded slots (waits for the later one). */
+int ek_mark(ek_ctx *ctx, int32_t slot);
+int ek_elapsed(ek_ctx *ctx, int32_t slot_a, int32_t slot_b, double *ms);
+/* Total number of kernels this context has launched. */
+int ek_launch_count(const ek_ctx *ctx, int64_t *out);
+
 #ifdef __cplusplus
 }
 #endif
