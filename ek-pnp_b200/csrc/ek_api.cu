@@ -243,6 +243,10 @@ int poisson_now(ek_ctx *c) {
 
 }  // namespace
 
+namespace ek {
+void set_last_error(const char *msg) { g_err = msg; }
+}  // namespace ek
+
 // ---- residual kernels (ek_residual.cu) ----
 namespace ek {
 cudaError_t launch_residual_f64(const Chan &c, const double *fields, double *snap, double *part,

@@ -82,7 +82,12 @@ struct PoissonPlan {
 };
 // pass 0: row FFTs, 1: tridiagonal column solve, 2: inverse row FFTs + walls
 cudaError_t poisson_pass_f64(int pass, const PoissonPlan &pp, const Chan &c, double *fields, cudaStream_t s);
+// Same passes with the right-hand side and psi planes given directly.
+cudaError_t poisson_pass_f64_at(int pass, const PoissonPlan &pp, const Chan &c, const double *rhs, double *psi,
+                                cudaStream_t s);
 size_t poisson_smem_bytes_f64(int nx);
+// Record an error message for ek_last_error() (ek_api.cu).
+void set_last_error(const char *msg);
 cudaError_t poisson_set_smem_limits();
 
 }  // namespace ek

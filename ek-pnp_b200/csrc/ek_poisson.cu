@@ -185,6 +185,16 @@ cudaError_t poisson_pass_f64(int pass, const PoissonPlan &pp, const Chan &c, dou
     return cudaGetLastError();
 }
 
+cudaError_t poisson_pass_f64_at(int pass, const PoissonPlan &pp, const Chan &c, const double *rhs, double *psi,
+                                cudaStream_t s) {
+    const size_t smem = poisson_smem_bytes_f64(pp.nx);
+    const int rows2 = (pp.n + 1) / 2;
+    if (pass == 0) fwd_rows<<<rows2, PTPB, smem, s>>>(pp, rhs, c.nxp);
+    else if (pass == 1) tridiag<<<(pp.nx / 2 + 1 + PTPB - 1) / PTPB, PTPB, 0, s>>>(pp);
+    else inv_rows<<<rows2, PTPB, smem, s>>>(pp, c, psi);
+    return cudaGetLastError();
+}
+
 cudaError_t poisson_set_smem_limits() {
     cudaError_t e = cudaFuncSetAttribute(fwd_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     if (e != cudaSuccess) return e;

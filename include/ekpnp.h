@@ -185,6 +185,24 @@ int ek_sync(ek_ctx *ctx);
  * nx), index = pitch*y + x. */
 int ek_field_pointers(ek_ctx *ctx, double **out8, int32_t *pitch);
 
+/* ---- Poisson solve without device allocation --------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory inside their time loop (the reference allocates and frees four
+ * buffers in every Poisson call, poisson.cu:182-207; a host program whose
+ * device memory belongs to its own pool, or is fully committed, cannot).
+ * Computes psi (and, if ex/ey are given, E = -grad psi) from c+ and c- for the
+ * channel described by p, exactly as ek_poisson does, with every scratch
+ * buffer in device arrays built into the library (10.9 MB per GPU, held until
+ * the process exits).  cp, cn, psi, ex, ey: device arrays of nx*ny doubles,
+ * index nx*y + x.  Uses nx, ny, dx, dy, lx, eps, f_charge, zeta_lo, zeta_hi of p.
+ * Limit: nx*ny <= 524288 nodes (nx a power of two <= 8192, or nx <= 2048);
+ * larger channels return EK_ERR_TOO_LARGE.  All calls on a GPU share the
+ * scratch: calls that overlap on the GPU race, so order them on one stream.
+ * The first call on a device looks up the scratch addresses; make it before
+ * any stream capture.  stream: a cudaStream_t, NULL for the legacy stream. */
+int ek_poisson_noalloc(const ek_params *p, const double *cp, const double *cn,
+                       double *psi, double *ex, double *ey, void *stream);
+
 /* ---- profiling (CUDA events on the context's stream) ------------------
  * Phases of a step: 0 = fused LBM kernel, 1 = Poisson pass A (row FFTs),
  * 2 = pass B (tridiagonal y-solve), 3 = pass C (inverse row FFTs).

@@ -1,0 +1,89 @@
+"""ek_poisson_noalloc against the allocating Poisson solve (ek_poisson).
+
+ek_poisson_noalloc exists for callers that cannot allocate device memory in
+their time loop -- the reference allocates four buffers in every Poisson call;
+a host program that owns all device memory through its own pool cannot.  Its
+scratch lives in device arrays built into the library.  This test calls it
+through the C ABI twice in a row, with different channels and charges, and
+checks psi, Ex and Ey against the allocating entry point at the tolerance of
+the other parity tests (1e-12 of the field's max-abs).  The second call
+checks that what the first call left in the shared scratch does not leak into
+the next result.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def allocating_solve(p, cp, cn):
+    import ekpnp
+    with ekpnp.Channel(p) as ch:
+        ch.set_fields(cp=cp, cn=cn)
+        ch.poisson()
+        return ch.get_fields(("psi", "ex", "ey"))
+
+
+def noalloc_solve(p, cp, cn):
+    import torch
+    import ekpnp
+    from ekpnp import EkParams, lib
+    dev = torch.device("cuda", 0)
+    tcp = torch.from_numpy(cp).to(dev)
+    tcn = torch.from_numpy(cn).to(dev)
+    out = {k: torch.full_like(tcp, float("nan")) for k in ("psi", "ex", "ey")}
+    torch.cuda.synchronize()
+    params = EkParams.from_dict(p)
+    rc = lib().ek_poisson_noalloc(ctypes.byref(params), ctypes.c_void_p(tcp.data_ptr()),
+                                  ctypes.c_void_p(tcn.data_ptr()), ctypes.c_void_p(out["psi"].data_ptr()),
+                                  ctypes.c_void_p(out["ex"].data_ptr()), ctypes.c_void_p(out["ey"].data_ptr()),
+                                  None)
+    ekpnp._lib.check(rc)
+    torch.cuda.synchronize()
+    return {k: v.cpu().numpy() for k, v in out.items()}
+
+
+def charges(nx, ny, seed, amp):
+    rng = np.random.default_rng(seed)
+    x = np.arange(nx)[None, :]
+    y = np.arange(ny)[:, None]
+    base = amp * np.sin(np.pi * y / (ny - 1)) * (1.0 + 0.3 * np.cos(2 * np.pi * x / nx))
+    cp = 1.0 + base + 1e-3 * rng.standard_normal((ny, nx))
+    cn = 1.0 - base + 1e-3 * rng.standard_normal((ny, nx))
+    return cp, cn
+
+
+def test_noalloc_matches_allocating_solve_twice():
+    import ekpnp
+    ekpnp.set_device(0)
+    calls = [
+        (ekpnp.channel_params(256, 128, kappa_h=8.0, zeta=-2.0), charges(256, 128, 1, 0.4)),
+        (ekpnp.channel_params(96, 61, kappa_h=3.0, zeta=-1.0, zeta_hi=-0.5), charges(96, 61, 2, 0.1)),
+    ]
+    for p, (cp, cn) in calls:
+        want = allocating_solve(p, cp, cn)
+        got = noalloc_solve(p, cp, cn)
+        for k in ("psi", "ex", "ey"):
+            assert np.all(np.isfinite(got[k])), k
+            assert rel_err(got[k], want[k]) <= 1e-12, (k, rel_err(got[k], want[k]))
+
+
+def test_noalloc_rejects_oversized_channel():
+    """2048 x 512 nodes is above the 524,288-node limit.  The buffers are real
+    and full-size, so the call is safe whatever it does; it must return
+    EK_ERR_TOO_LARGE and leave psi untouched."""
+    import torch
+    import ekpnp
+    from ekpnp import EkParams, lib
+    p = EkParams.from_dict(ekpnp.channel_params(2048, 512))
+    buf = [torch.zeros((512, 2048), dtype=torch.float64, device="cuda:0") for _ in range(3)]
+    torch.cuda.synchronize()
+    rc = lib().ek_poisson_noalloc(ctypes.byref(p), *[ctypes.c_void_p(b.data_ptr()) for b in buf],
+                                  None, None, None)
+    torch.cuda.synchronize()
+    assert rc == 7  # EK_ERR_TOO_LARGE
+    assert float(buf[2].abs().max()) == 0.0
