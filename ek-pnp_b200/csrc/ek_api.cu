@@ -6,10 +6,14 @@
 // poisson.cu; every failure is returned as a status instead of exit().
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <string>
+#include <thread>
+#include <utility>
 #include <vector>
 
 #include "ek_internal.h"
@@ -56,6 +60,7 @@ struct ek_ctx {
     bool e_stale = false;      // E planes older than psi
     double *fields = nullptr;
     double *wall = nullptr;    // 6 x nx
+    std::vector<double> wall_host;  // host copy of the wall profiles
     double *snap = nullptr;    // residual snapshot, 4 planes
     double *part = nullptr;    // residual partial sums
     bool snap_valid = false;
@@ -241,6 +246,48 @@ int poisson_now(ek_ctx *c) {
     return EK_OK;
 }
 
+// Discrete 1D Poisson-Boltzmann equation down one column (rows 1..ny-2):
+//   (psi_{j-1} - 2 psi_j + psi_{j+1})/dy^2 + g (exp(-a psi_j) - exp(a psi_j)) = 0
+// with psi_0 = zl, psi_{ny-1} = zh, g = f_charge c0/eps, a = e/kT.  Damped
+// Newton from the linear profile; each step changes a*psi by at most 1.
+bool pb_column(int ny, double dy, double g, double a, double zl, double zh, std::vector<double> &psi) {
+    psi.assign(ny, 0.0);
+    for (int j = 0; j < ny; ++j) psi[j] = zl + (zh - zl) * (double)j / (double)(ny - 1);
+    const int n = ny - 2;
+    const double inv = 1.0 / (dy * dy);
+    std::vector<double> rhs(n), diag(n), cp(n), dp(n);
+    const double scale = std::max({std::fabs(zl), std::fabs(zh), 1.0});
+    int polish = -1;  // full Newton steps left once the update is small
+    for (int it = 0; it < 500; ++it) {
+        double gmax = 0.0;
+        for (int j = 0; j < n; ++j) {
+            const double v = psi[j + 1], em = std::exp(-a * v), ep = std::exp(a * v);
+            const double G = (psi[j] - 2.0 * v + psi[j + 2]) * inv + g * (em - ep);
+            rhs[j] = -G;
+            diag[j] = -2.0 * inv - g * a * (em + ep);
+            gmax = std::max(gmax, std::fabs(G));
+        }
+        // Thomas solve of J delta = -G (off-diagonals inv)
+        cp[0] = inv / diag[0];
+        dp[0] = rhs[0] / diag[0];
+        for (int j = 1; j < n; ++j) {
+            const double den = diag[j] - inv * cp[j - 1];
+            cp[j] = inv / den;
+            dp[j] = (rhs[j] - inv * dp[j - 1]) / den;
+        }
+        for (int j = n - 2; j >= 0; --j) dp[j] -= cp[j] * dp[j + 1];
+        double dmax = 0.0;
+        for (int j = 0; j < n; ++j) dmax = std::max(dmax, std::fabs(a * dp[j]));
+        const double damp = dmax > 1.0 ? 1.0 / dmax : 1.0;
+        for (int j = 0; j < n; ++j) psi[j + 1] += damp * dp[j];
+        (void)gmax;
+        // quadratic convergence: two more full steps after |a delta| < 1e-9 reach rounding
+        if (polish < 0 && damp == 1.0 && dmax < 1e-9 * scale) polish = 2;
+        if (polish >= 0 && polish-- == 0) return true;
+    }
+    return false;
+}
+
 }  // namespace
 
 namespace ek {
@@ -352,6 +399,7 @@ int ek_create(const ek_params *p, ek_ctx **out) {
         for (int x = 0; x < p->nx; ++x) wall[(size_t)k * p->nx + x] = uni[k];
     std::vector<double> piv = make_pivots(*p, c->n, c->mp);
     std::vector<double2> tw = make_twiddles(p->nx);
+    c->wall_host = wall;
     e = cudaMemcpyAsync(c->wall, wall.data(), wall.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(c->pp.piv, piv.data(), piv.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(c->pp.tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream);
@@ -426,8 +474,80 @@ int ek_set_wall_profile(ek_ctx *c, const double *zlo, const double *zhi, const d
         EK_CUDA(cudaMemcpyAsync(c->wall + (size_t)k * c->p.nx, src[k], c->p.nx * sizeof(double),
                                 cudaMemcpyHostToDevice, c->stream),
                 "copy wall profile");
+        std::copy(src[k], src[k] + c->p.nx, c->wall_host.begin() + (size_t)k * c->p.nx);
     }
     EK_CUDA(cudaStreamSynchronize(c->stream), "wall profile sync");
+    return EK_OK;
+}
+
+int ek_init_poisson_boltzmann(ek_ctx *c, int32_t method, int32_t iterations, double omega, double e_kt) {
+    if (!c) return fail(EK_ERR_INVALID, "null context");
+    if (!std::isfinite(e_kt) || e_kt == 0.0) return fail(EK_ERR_INVALID, "e_kt must be finite and non-zero");
+    const ek_params &p = c->p;
+    if (method == EK_PB_REFERENCE) {
+        if (iterations < 0 || !(omega > 0.0) || !(omega <= 1.0)) return fail(EK_ERR_INVALID, "need iterations >= 0, 0 < omega <= 1");
+        double *old = nullptr;
+        EK_CUDA(cudaMalloc(&old, c->plane * sizeof(double)), "PB scratch");
+        int rc = EK_OK;
+        auto run = [&]() -> int {
+            EK_CUDA(launch_pb_fill(c->chan, c->fields, old, c->stream), "PB fill");
+            for (int32_t it = 0; it < iterations; ++it) {
+                EK_CUDA(launch_pb_conc(c->chan, e_kt, c->fields, c->stream), "PB concentrations");
+                EK_CUDA(launch_rhs_from_moments_f64(c->chan, c->fields, c->stream), "rhs kernel");
+                for (int pass = 0; pass < 3; ++pass)
+                    EK_CUDA(poisson_pass_f64(pass, c->pp, c->chan, c->fields, c->stream), "poisson kernel");
+                EK_CUDA(launch_efield_f64(c->chan, c->fields, c->stream), "efield kernel");
+                EK_CUDA(launch_pb_relax(c->chan, omega, c->fields, old, c->stream), "PB relax");
+            }
+            EK_CUDA(cudaStreamSynchronize(c->stream), "PB sync");
+            return EK_OK;
+        };
+        rc = run();
+        cudaFree(old);
+        if (rc != EK_OK) return rc;
+        // the fields now hold E of the last Poisson solve, as the reference's do
+        c->explicit_e_once = iterations > 0;
+        c->e_stale = iterations == 0;
+        return EK_OK;
+    }
+    if (method != EK_PB_NEWTON) return fail(EK_ERR_INVALID, "unknown Poisson-Boltzmann method");
+    const int nx = p.nx, ny = p.ny;
+    const double g = p.f_charge * p.c0 / p.eps;
+    // one Newton solve per distinct pair of wall potentials
+    std::map<std::pair<double, double>, std::vector<double>> prof;
+    for (int x = 0; x < nx; ++x) prof[{c->wall_host[x], c->wall_host[nx + x]}];
+    std::vector<std::pair<const std::pair<double, double>, std::vector<double>> *> work;
+    for (auto &kv : prof) work.push_back(&kv);
+    std::vector<int> ok(work.size(), 1);
+    const unsigned nt = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), (unsigned)work.size()));
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < nt; ++t)
+        pool.emplace_back([&, t] {
+            for (size_t i = t; i < work.size(); i += nt)
+                ok[i] = pb_column(ny, p.dy, g, e_kt, work[i]->first.first, work[i]->first.second, work[i]->second);
+        });
+    for (auto &th : pool) th.join();
+    for (int v : ok)
+        if (!v) return fail(EK_ERR_INVALID, "Poisson-Boltzmann Newton iteration did not converge");
+    std::vector<double> rho((size_t)nx * ny, p.rho0), zero((size_t)nx * ny, 0.0), psi((size_t)nx * ny),
+        cpv((size_t)nx * ny), cnv((size_t)nx * ny);
+    for (int x = 0; x < nx; ++x) {
+        const std::vector<double> &col = prof[{c->wall_host[x], c->wall_host[nx + x]}];
+        for (int y = 0; y < ny; ++y) {
+            const size_t k = (size_t)y * nx + x;
+            psi[k] = col[y];
+            cpv[k] = p.c0 * std::exp(-e_kt * col[y]);
+            cnv[k] = p.c0 * std::exp(e_kt * col[y]);
+        }
+    }
+    const double *src[F_RHS] = {rho.data(), zero.data(), zero.data(), cpv.data(), cnv.data(), psi.data(), nullptr, nullptr};
+    for (int k = 0; k < F_RHS; ++k) {
+        int rc = copy_in(c, k, src[k]);
+        if (rc != EK_OK) return rc;
+    }
+    EK_CUDA(cudaStreamSynchronize(c->stream), "PB upload");
+    c->explicit_e_once = false;
+    c->e_stale = true;
     return EK_OK;
 }
 

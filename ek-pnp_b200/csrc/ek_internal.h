@@ -64,6 +64,11 @@ cudaError_t launch_step_f64(const Chan &c, const double *src, double *dst, doubl
 cudaError_t launch_efield_f64(const Chan &c, double *fields, cudaStream_t s);
 cudaError_t launch_rhs_from_moments_f64(const Chan &c, double *fields, cudaStream_t s);
 
+// ---- Poisson-Boltzmann start (ek_init.cu) ----
+cudaError_t launch_pb_fill(const Chan &c, double *fields, double *psi_old, cudaStream_t s);
+cudaError_t launch_pb_conc(const Chan &c, double e_kt, double *fields, cudaStream_t s);
+cudaError_t launch_pb_relax(const Chan &c, double omega, double *fields, double *psi_old, cudaStream_t s);
+
 // ---- shifted-storage forms (ek_lbm_f32.cu); storage = EK_STORE_F32 or _F16 ----
 cudaError_t launch_step_shifted(const Chan &c, int storage, const void *src, void *dst, double *fields,
                                 bool first, bool explicit_e, bool moments, cudaStream_t s);

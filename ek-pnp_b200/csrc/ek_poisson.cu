@@ -11,9 +11,11 @@
 // and this file solves it directly (Thomas recurrence with pivots computed
 // once per channel), for any ny, with no FFT in y:
 //   pass A  per pair of interior rows: real FFT in x (two rows packed as one
-//           complex row, radix-2 in shared memory; direct DFT when nx is not
-//           a power of two) -> spec[j][m], m = 0..nx/2
-//   pass B  per x-mode m: forward/backward Thomas sweep down the column
+//           complex row; register-blocked radix-16 passes for powers of two,
+//           direct DFT otherwise) -> spec[j][m], m = 0..nx/2
+//   pass B  per x-mode m: Thomas sweeps down the column, partitioned into row
+//           segments of at most 16 rows held in registers (one thread per
+//           mode for columns taller than 8192 rows)
 //   pass C  per pair of rows: inverse real FFT -> psi; wall rows = zeta(x)
 // The result equals the reference's to rounding (the test suite compares).
 #include <cuda_runtime.h>
@@ -169,6 +171,313 @@ inv_rows(const PoissonPlan pp, const Chan c, double *__restrict__ psi) {
     }
 }
 
+// ---- register-blocked radix-16 row FFTs (power-of-two nx >= 16) ----------
+//
+// Each thread holds up to 16 complex values and runs up to four radix-2
+// stages on them in registers per pass; passes exchange through shared
+// memory.  The forward transform is decimation in frequency on natural-order
+// input (bit-reversed output); the inverse is decimation in time on
+// bit-reversed input (natural-order output).  A pass over index bits
+// [b, b+RB) owns the 2^RB elements that share every other index bit; thread t
+// of the T = nx/16 threads of one transform owns 16/2^RB such groups.
+// Twiddle of stage st for element index i: exp(-2 pi i (i mod 2^st)/2^(st+1))
+// = A * C with A = exp(-2 pi i (base mod 2^b)/2^(st+1)) from the table (one
+// load per group and stage) and C = exp(-2 pi i v_low/2^(st-b+1)) a constant
+// root of unity of order <= 16 for the in-register index bits v_low.
+// Shared memory is addressed through swz(): the low three index bits are
+// XOR-ed with bits 4..6 and with the reversed top three bits, which keeps
+// both the passes and the bit-reversed unpacking free of bank conflicts.
+
+__device__ __forceinline__ int brev(int i, int lg) { return (int)(__brev((unsigned)i) >> (32 - lg)); }
+__device__ __forceinline__ int swz(int i, int k) {
+    if (k < 6) return i;
+    const int top = (i >> (k - 3)) & 7;
+    const int rtop = ((top & 1) << 2) | (top & 2) | ((top >> 2) & 1);
+    return i ^ (((i >> 4) ^ rtop) & 7);
+}
+
+// exp(-2 pi i v/2^(sl+1)) for 0 <= v < 2^sl <= 8 (compile-time arguments)
+__device__ __forceinline__ double2 root16(int sl, int v) {
+    const int q = v << (3 - sl);  // angle = q * pi/8
+    switch (q) {
+        case 0: return make_double2(1.0, 0.0);
+        case 1: return make_double2(0.92387953251128674, -0.38268343236508977);
+        case 2: return make_double2(0.70710678118654752, -0.70710678118654752);
+        case 3: return make_double2(0.38268343236508977, -0.92387953251128674);
+        case 4: return make_double2(0.0, -1.0);
+        case 5: return make_double2(-0.38268343236508977, -0.92387953251128674);
+        case 6: return make_double2(-0.70710678118654752, -0.70710678118654752);
+        default: return make_double2(-0.92387953251128674, -0.38268343236508977);
+    }
+}
+
+template <bool INV, int RB>
+__device__ __forceinline__ void reg_pass(double2 *s, int k, int T, int t, int b, const double2 *__restrict__ tw) {
+    constexpr int G = 16 >> RB, E = 1 << RB;
+    const int ngroups = (1 << k) >> RB;
+#pragma unroll
+    for (int q = 0; q < G; ++q) {
+        const int g = t + q * T;
+        if (g >= ngroups) continue;
+        const int kb = g & ((1 << b) - 1);
+        const int base = kb | ((g >> b) << (b + RB));
+        double2 r[E];
+#pragma unroll
+        for (int v = 0; v < E; ++v) r[v] = s[swz(base | (v << b), k)];
+        if (!INV) {
+#pragma unroll
+            for (int sl = RB - 1; sl >= 0; --sl) {
+                const int st = b + sl;
+                const double2 A = __ldg(tw + (kb << (k - st - 1)));
+#pragma unroll
+                for (int v = 0; v < E; ++v) {
+                    if (v & (1 << sl)) continue;
+                    const double2 w = cmul(A, root16(sl, v & ((1 << sl) - 1)));
+                    const double2 u = r[v], x = r[v + (1 << sl)];
+                    r[v] = cadd(u, x);
+                    r[v + (1 << sl)] = cmul(csub(u, x), w);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int sl = 0; sl < RB; ++sl) {
+                const int st = b + sl;
+                const double2 A = cconj(__ldg(tw + (kb << (k - st - 1))));
+#pragma unroll
+                for (int v = 0; v < E; ++v) {
+                    if (v & (1 << sl)) continue;
+                    const double2 w = cmul(A, cconj(root16(sl, v & ((1 << sl) - 1))));
+                    const double2 u = r[v], x = cmul(r[v + (1 << sl)], w);
+                    r[v] = cadd(u, x);
+                    r[v + (1 << sl)] = csub(u, x);
+                }
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < E; ++v) s[swz(base | (v << b), k)] = r[v];
+    }
+}
+
+template <bool INV>
+__device__ __forceinline__ void reg_pass_any(double2 *s, int k, int T, int t, int b, int rb, const double2 *tw) {
+    switch (rb) {
+        case 4: reg_pass<INV, 4>(s, k, T, t, b, tw); break;
+        case 3: reg_pass<INV, 3>(s, k, T, t, b, tw); break;
+        case 2: reg_pass<INV, 2>(s, k, T, t, b, tw); break;
+        default: reg_pass<INV, 1>(s, k, T, t, b, tw); break;
+    }
+}
+
+// Whole transform of 2^k points in s; every thread of the block calls it.
+template <bool INV>
+__device__ void reg_fft(double2 *s, int k, int T, int t, const double2 *__restrict__ tw) {
+    if (!INV) {
+        for (int top = k; top > 0;) {
+            const int rb = top < 4 ? top : 4;
+            reg_pass_any<false>(s, k, T, t, top - rb, rb, tw);
+            __syncthreads();
+            top -= rb;
+        }
+    } else {
+        for (int b = 0; b < k;) {
+            const int rb = k - b < 4 ? k - b : 4;
+            reg_pass_any<true>(s, k, T, t, b, rb, tw);
+            __syncthreads();
+            b += rb;
+        }
+    }
+}
+
+// Pass A, radix-16 form: row pairs (2p+1, 2p+2) of the right-hand side ->
+// spectra.  One block holds BLOCK/T row pairs.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 512 / BLOCK)
+fwd_rows_r16(const PoissonPlan pp, const double *__restrict__ rhs, int nxp) {
+    extern __shared__ double2 sm[];
+    const int N = pp.nx, k = pp.log2nx, T = N >> 4;
+    const int per = BLOCK / T;
+    const int p = threadIdx.x / T, t = threadIdx.x - p * T;
+    const int pair = blockIdx.x * per + p;
+    double2 *s = sm + p * N;
+    const int j0 = 2 * pair, j1 = j0 + 1;
+    const bool live = j0 < pp.n, two = j1 < pp.n;
+    const double *r0 = rhs + (size_t)(j0 + 1) * nxp, *r1 = rhs + (size_t)(j1 + 1) * nxp;
+    for (int x = t; x < N; x += T)
+        s[swz(x, k)] = live ? make_double2(__ldg(r0 + x), two ? __ldg(r1 + x) : 0.0) : make_double2(0.0, 0.0);
+    __syncthreads();
+    reg_fft<false>(s, k, T, t, pp.tw);
+    if (!live) return;
+    double2 *s0 = pp.spec + (size_t)j0 * pp.mp, *s1 = pp.spec + (size_t)j1 * pp.mp;
+    for (int m = t; m <= N / 2; m += T) {
+        const double2 a = s[swz(brev(m, k), k)], b = cconj(s[swz(brev((N - m) & (N - 1), k), k)]);
+        s0[m] = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y + b.y));
+        if (two) s1[m] = make_double2(0.5 * (a.y - b.y), -0.5 * (a.x - b.x));
+    }
+}
+
+// Pass C, radix-16 form: spectra -> psi rows; block 0 also writes the walls.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 512 / BLOCK)
+inv_rows_r16(const PoissonPlan pp, const Chan c, double *__restrict__ psi) {
+    extern __shared__ double2 sm[];
+    const int N = pp.nx, k = pp.log2nx, T = N >> 4;
+    const int per = BLOCK / T;
+    const int p = threadIdx.x / T, t = threadIdx.x - p * T;
+    const int pair = blockIdx.x * per + p;
+    double2 *s = sm + p * N;
+    const int j0 = 2 * pair, j1 = j0 + 1;
+    const bool live = j0 < pp.n, two = j1 < pp.n;
+    const double2 *s0 = pp.spec + (size_t)j0 * pp.mp, *s1 = pp.spec + (size_t)j1 * pp.mp;
+    for (int m = t; m <= N / 2; m += T) {
+        const double2 a = live ? s0[m] : make_double2(0.0, 0.0);
+        const double2 b = two ? s1[m] : make_double2(0.0, 0.0);
+        s[swz(brev(m, k), k)] = make_double2(a.x - b.y, a.y + b.x);  // A + iB
+        if (m != 0 && 2 * m != N) s[swz(brev(N - m, k), k)] = make_double2(a.x + b.y, -a.y + b.x);
+    }
+    __syncthreads();
+    reg_fft<true>(s, k, T, t, pp.tw);
+    const double inv = 1.0 / (double)N;
+    if (live) {
+        double *p0 = psi + (size_t)(j0 + 1) * c.nxp, *p1 = psi + (size_t)(j1 + 1) * c.nxp;
+        for (int x = t; x < N; x += T) {
+            const double2 z = s[swz(x, k)];
+            p0[x] = z.x * inv;
+            if (two) p1[x] = z.y * inv;
+        }
+    }
+    if (blockIdx.x == 0) {
+        double *lo = psi, *hi = psi + (size_t)(c.ny - 1) * c.nxp;
+        for (int x = threadIdx.x; x < N; x += BLOCK) {
+            lo[x] = c.zlo[x];
+            hi[x] = c.zhi[x];
+        }
+    }
+}
+
+// ---- pass B, partitioned Thomas solve ------------------------------------
+//
+// A block owns M consecutive x-modes; its 512 threads are S = 512/M row
+// segments x M modes, each segment at most 16 rows (M is chosen so), held in
+// registers with its pivots.  The forward recurrence
+// d_j = (dy^2 S_j - d_{j-1}) piv_j is linear in the value entering a segment,
+// so each segment first runs with a zero entry value while accumulating the
+// product of (-piv); one thread per mode then carries the true entry values
+// across the S segments through shared memory, and each segment adds its
+// correction.  The backward recurrence x_j = d_j - piv_j x_{j+1} is split the
+// same way.  The result is the Thomas solution, reassociated.
+constexpr int TB_THREADS = 512;
+constexpr int TB_L = 16;
+
+__global__ void __launch_bounds__(TB_THREADS) tridiag_part(const PoissonPlan pp, int M) {
+    __shared__ double2 ends[TB_THREADS];
+    __shared__ double mults[TB_THREADS];
+    __shared__ double2 carry[TB_THREADS];
+    const int n = pp.n, mlast = pp.nx / 2;
+    const size_t mp = pp.mp;
+    const int tid = threadIdx.x, mode = tid % M, seg = tid / M, S = TB_THREADS / M;
+    const int m = blockIdx.x * M + mode;
+    const bool mvalid = m <= mlast;
+    const int L = (n + S - 1) / S, ja = seg * L, cnt = max(0, min(n, ja + L) - ja);
+    double c[TB_L];
+    double2 v[TB_L];
+    const double dy2 = pp.dy2;
+#pragma unroll
+    for (int q = 0; q < TB_L; ++q) {
+        const bool on = mvalid && q < cnt;
+        c[q] = on ? __ldg(pp.piv + (size_t)(ja + q) * mp + m) : 0.0;
+        const double2 sv = on ? pp.spec[(size_t)(ja + q) * mp + m] : make_double2(0.0, 0.0);
+        v[q] = make_double2(dy2 * sv.x, dy2 * sv.y);
+    }
+    double2 d = make_double2(0.0, 0.0);
+    double mu = 1.0;
+#pragma unroll
+    for (int q = 0; q < TB_L; ++q) {
+        if (q < cnt) {
+            d = make_double2((v[q].x - d.x) * c[q], (v[q].y - d.y) * c[q]);
+            mu = -c[q] * mu;
+            v[q] = d;
+        }
+    }
+    ends[tid] = d;
+    mults[tid] = mu;
+    __syncthreads();
+    if (seg == 0) {  // true entry value of every segment
+        double2 D = make_double2(0.0, 0.0);
+        for (int s_ = 0; s_ < S; ++s_) {
+            carry[s_ * M + mode] = D;
+            const double2 e = ends[s_ * M + mode];
+            const double f = mults[s_ * M + mode];
+            D = make_double2(e.x + f * D.x, e.y + f * D.y);
+        }
+    }
+    __syncthreads();
+    {
+        const double2 D = carry[tid];
+        mu = 1.0;
+#pragma unroll
+        for (int q = 0; q < TB_L; ++q) {
+            if (q < cnt) {
+                mu = -c[q] * mu;
+                v[q].x += mu * D.x;
+                v[q].y += mu * D.y;
+            }
+        }
+    }
+    double2 x = make_double2(0.0, 0.0);
+    double nu = 1.0;
+#pragma unroll
+    for (int q = TB_L - 1; q >= 0; --q) {
+        if (q < cnt) {
+            x = make_double2(v[q].x - c[q] * x.x, v[q].y - c[q] * x.y);
+            nu = -c[q] * nu;
+            v[q] = x;
+        }
+    }
+    __syncthreads();  // carries of the forward sweep are no longer read
+    ends[tid] = x;
+    mults[tid] = nu;
+    __syncthreads();
+    if (seg == 0) {  // true exit value of every segment (x_n = 0)
+        double2 X = make_double2(0.0, 0.0);
+        for (int s_ = S - 1; s_ >= 0; --s_) {
+            carry[s_ * M + mode] = X;
+            const double2 e = ends[s_ * M + mode];
+            const double f = mults[s_ * M + mode];
+            X = make_double2(e.x + f * X.x, e.y + f * X.y);
+        }
+    }
+    __syncthreads();
+    if (!mvalid) return;
+    const double2 X = carry[tid];
+    nu = 1.0;
+#pragma unroll
+    for (int q = TB_L - 1; q >= 0; --q) {
+        if (q < cnt) {
+            nu = -c[q] * nu;
+            pp.spec[(size_t)(ja + q) * mp + m] = make_double2(v[q].x + nu * X.x, v[q].y + nu * X.y);
+        }
+    }
+}
+
+// Modes per block of tridiag_part for n rows, so that every segment has at
+// most TB_L rows (0: too tall, use the one-thread-per-mode `tridiag`).
+int tridiag_modes(int n) {
+    for (int M = 8; M >= 1; M >>= 1)
+        if ((n + TB_THREADS / M - 1) / (TB_THREADS / M) <= TB_L) return M;
+    return 0;
+}
+
+bool use_r16(const PoissonPlan &pp) { return pp.pow2 && pp.nx >= 16; }
+
+// Threads per block and row pairs per block of the radix-16 row kernels.
+void r16_shape(int nx, int *threads, int *per) {
+    const int T = nx >> 4;
+    *threads = T >= 256 ? T : 256;
+    *per = *threads / T;
+}
+
+size_t r16_smem(int nx, int per) { return (size_t)per * nx * sizeof(double2); }
+
 }  // namespace
 
 size_t poisson_smem_bytes_f64(int nx) {
@@ -177,28 +486,49 @@ size_t poisson_smem_bytes_f64(int nx) {
 }
 
 cudaError_t poisson_pass_f64(int pass, const PoissonPlan &pp, const Chan &c, double *fields, cudaStream_t s) {
-    const size_t smem = poisson_smem_bytes_f64(pp.nx);
-    const int rows2 = (pp.n + 1) / 2;
-    if (pass == 0) fwd_rows<<<rows2, PTPB, smem, s>>>(pp, fields + F_RHS * c.plane, c.nxp);
-    else if (pass == 1) tridiag<<<(pp.nx / 2 + 1 + PTPB - 1) / PTPB, PTPB, 0, s>>>(pp);
-    else inv_rows<<<rows2, PTPB, smem, s>>>(pp, c, fields + F_PSI * c.plane);
-    return cudaGetLastError();
+    return poisson_pass_f64_at(pass, pp, c, fields + F_RHS * c.plane, fields + F_PSI * c.plane, s);
 }
 
 cudaError_t poisson_pass_f64_at(int pass, const PoissonPlan &pp, const Chan &c, const double *rhs, double *psi,
                                 cudaStream_t s) {
-    const size_t smem = poisson_smem_bytes_f64(pp.nx);
     const int rows2 = (pp.n + 1) / 2;
+    if (pass == 1) {
+        const int M = tridiag_modes(pp.n);
+        if (M > 0) tridiag_part<<<(pp.nx / 2 + M) / M, TB_THREADS, 0, s>>>(pp, M);
+        else tridiag<<<(pp.nx / 2 + 1 + PTPB - 1) / PTPB, PTPB, 0, s>>>(pp);
+        return cudaGetLastError();
+    }
+    if (use_r16(pp)) {
+        int threads, per;
+        r16_shape(pp.nx, &threads, &per);
+        const size_t smem = r16_smem(pp.nx, per);
+        const int blocks = (rows2 + per - 1) / per;
+        if (threads == 256) {
+            if (pass == 0) fwd_rows_r16<256><<<blocks, 256, smem, s>>>(pp, rhs, c.nxp);
+            else inv_rows_r16<256><<<blocks, 256, smem, s>>>(pp, c, psi);
+        } else {
+            if (pass == 0) fwd_rows_r16<512><<<blocks, 512, smem, s>>>(pp, rhs, c.nxp);
+            else inv_rows_r16<512><<<blocks, 512, smem, s>>>(pp, c, psi);
+        }
+        return cudaGetLastError();
+    }
+    const size_t smem = poisson_smem_bytes_f64(pp.nx);
     if (pass == 0) fwd_rows<<<rows2, PTPB, smem, s>>>(pp, rhs, c.nxp);
-    else if (pass == 1) tridiag<<<(pp.nx / 2 + 1 + PTPB - 1) / PTPB, PTPB, 0, s>>>(pp);
     else inv_rows<<<rows2, PTPB, smem, s>>>(pp, c, psi);
     return cudaGetLastError();
 }
 
 cudaError_t poisson_set_smem_limits() {
-    cudaError_t e = cudaFuncSetAttribute(fwd_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(inv_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    const void *fns[] = {(const void *)fwd_rows, (const void *)inv_rows, (const void *)fwd_rows_r16<256>,
+                         (const void *)inv_rows_r16<256>, (const void *)fwd_rows_r16<512>,
+                         (const void *)inv_rows_r16<512>};
+    for (const void *f : fns) {
+        cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 }  // namespace ek

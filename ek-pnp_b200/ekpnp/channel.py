@@ -86,6 +86,13 @@ class Channel:
             arrs.append(a)
         check(lib().ek_set_wall_profile(self._h, *[_ptr(a) for a in arrs]))
 
+    def init_poisson_boltzmann(self, method="newton", iterations=501, omega=0.05, e_kt=1.0):
+        """Poisson-Boltzmann fields (u = 0).  method "reference" is the
+        reference's own under-relaxed iteration (LBM.cu:95-145); "newton" a
+        damped Newton solve per x-column."""
+        m = {"reference": 0, "newton": 1}[method]
+        check(lib().ek_init_poisson_boltzmann(self._h, m, int(iterations), float(omega), float(e_kt)))
+
     def init_equilibrium(self):
         check(lib().ek_init_equilibrium(self._h))
 

@@ -141,6 +141,22 @@ int ek_set_wall_profile(ek_ctx *ctx, const double *zeta_lo, const double *zeta_h
                         const double *cp_lo, const double *cp_hi,
                         const double *cn_lo, const double *cn_hi);
 
+/* Poisson-Boltzmann start: sets rho = rho0, u = 0, c+- = c0 exp(-+ e_kt psi)
+ * and psi (E follows from psi).  e_kt is e/kT in the units of psi (1 when psi
+ * is in thermal volts).
+ *   method EK_PB_REFERENCE: the reference's own start (initialization,
+ *     LBM.cu:95-145): psi = zeta_lo everywhere, then `iterations` rounds of
+ *     {c+- from psi, Poisson solve, psi = omega psi + (1-omega) psi_old}.  It
+ *     converges only for weak coupling (roughly kappa*H below 10 at |zeta| = 2).
+ *   method EK_PB_NEWTON: damped Newton iteration of the discrete 1D
+ *     Poisson-Boltzmann equation down every x-column (rows 1..ny-2, Dirichlet
+ *     wall values), iterations/omega ignored.  Exact for walls uniform in x,
+ *     the column-local solution otherwise.
+ * Follow with ek_init_equilibrium (optionally after perturbing the fields). */
+enum { EK_PB_REFERENCE = 0, EK_PB_NEWTON = 1 };
+int ek_init_poisson_boltzmann(ek_ctx *ctx, int32_t method, int32_t iterations,
+                              double omega, double e_kt);
+
 /* Populations at equilibrium with the loaded fields: init_equilibrium /
  * gpu_init_equilibrium (LBM.cu:183-305). */
 int ek_init_equilibrium(ek_ctx *ctx);

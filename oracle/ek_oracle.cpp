@@ -560,6 +560,34 @@ int ekor_set_wall_profile(ekor *s, const double *zlo, const double *zhi, const d
     return EK_OK;
 }
 
+// Poisson-Boltzmann start, LBM.cu:95-145: fields of gpu_initialization
+// (rho0, u = 0, psi = voltage everywhere, E = 0), then `iters` rounds of
+// {c+- = c0 exp(-+ e_kt psi) (gpu_PBE), fast_Poisson, psi = omega psi +
+// (1 - omega) psi_old (gpu_PBE_phi)}.  E keeps the last Poisson result.
+int ekor_init_pb(ekor *s, int iters, double omega, double e_kt) {
+    if (!s || iters < 0) return EK_ERR_INVALID;
+    const size_t nn = s->nn;
+    for (size_t k = 0; k < nn; ++k) {
+        s->rho[k] = s->p.rho0;
+        s->ux[k] = s->uy[k] = 0.0;
+        s->psi[k] = s->zlo[k % s->nx];
+        s->ex[k] = s->ey[k] = 0.0;
+    }
+    std::vector<double> old(s->psi);
+    for (int it = 0; it < iters; ++it) {
+        for (size_t k = 0; k < nn; ++k) {
+            s->cp[k] = s->p.c0 * std::exp(-e_kt * s->psi[k]);
+            s->cn[k] = s->p.c0 * std::exp(e_kt * s->psi[k]);
+        }
+        poisson(*s);
+        for (size_t k = 0; k < nn; ++k) {
+            s->psi[k] = omega * s->psi[k] + (1.0 - omega) * old[k];
+            old[k] = s->psi[k];
+        }
+    }
+    return EK_OK;
+}
+
 int ekor_init_equilibrium(ekor *s) {
     if (!s) return EK_ERR_INVALID;
     init_equilibrium(*s);

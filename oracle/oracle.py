@@ -62,6 +62,7 @@ def lib():
         h.ekor_poisson.argtypes = [vp]
         h.ekor_get_fields.argtypes = [vp] + [dp] * 8
         h.ekor_get_populations.argtypes = [vp, dp, dp, dp]
+        h.ekor_init_pb.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double]
         _lib = h
     return _lib
 
@@ -108,6 +109,9 @@ class OracleChannel:
 
     def init_equilibrium(self):
         lib().ekor_init_equilibrium(self._h)
+
+    def init_poisson_boltzmann(self, iterations=501, omega=0.05, e_kt=1.0):
+        lib().ekor_init_pb(self._h, int(iterations), float(omega), float(e_kt))
 
     def step(self, n=1):
         lib().ekor_step(self._h, int(n))
