@@ -64,6 +64,10 @@ struct ek_ctx {
     double *snap = nullptr;    // residual snapshot, 4 planes
     double *part = nullptr;    // residual partial sums
     bool snap_valid = false;
+    float *kref[2] = {nullptr, nullptr};  // shifted storage: row references /36, double-buffered
+    int kcur = 0;
+    int kq[3] = {0, 0, 0};                // binary exponents of the reference grids
+    int32_t rebase_every = 0;
     Rates *rates_dev = nullptr;
     Rates rates{};
     PoissonPlan pp{};
@@ -111,6 +115,8 @@ void free_ctx(ek_ctx *c) {
     cudaFree(c->snap);
     cudaFree(c->part);
     cudaFree(c->rates_dev);
+    cudaFree(c->kref[0]);
+    cudaFree(c->kref[1]);
     cudaFree(c->pp.tw);
     cudaFree(c->pp.piv);
     cudaFree(c->pp.spec);
@@ -177,6 +183,36 @@ void refresh_chan(ek_ctx *c) {
     h.cphi = c->wall + 3 * p.nx;
     h.cnlo = c->wall + 4 * p.nx;
     h.cnhi = c->wall + 5 * p.nx;
+    h.kref = c->kref[c->kcur];
+}
+
+// Binary exponent q of a reference grid K 2^-q (values stored /36) for
+// values up to vmax: 36 K stays below 2^22, so 36 K 2^-q and every
+// (16|4|1) (K' - K) 2^-q are exact in FP32.
+int ref_exponent(double vmax) {
+    int e = 1;
+    while ((double)(1 << e) < vmax && e < 20) ++e;
+    return 22 - e;
+}
+
+int shifted(const ek_ctx *c) { return c->p.storage != EK_STORE_F64; }
+
+// New reference profile from the fields' row means into the spare buffer.
+int refs_from_fields(ek_ctx *c, float *out) {
+    EK_CUDA(launch_row_refs(c->chan, c->fields, c->kq[0], c->kq[1], c->kq[2], out, c->stream), "row refs");
+    ++c->launches;
+    return EK_OK;
+}
+
+int rebase_now(ek_ctx *c) {
+    float *kold = c->kref[c->kcur], *knew = c->kref[c->kcur ^ 1];
+    int rc = refs_from_fields(c, knew);
+    if (rc != EK_OK) return rc;
+    EK_CUDA(launch_rebase(c->chan, c->p.storage, c->pops[c->cur], kold, knew, c->stream), "rebase");
+    ++c->launches;
+    c->kcur ^= 1;
+    refresh_chan(c);
+    return EK_OK;
 }
 
 int copy_in(ek_ctx *c, int plane_idx, const double *src) {
@@ -386,6 +422,8 @@ int ek_create(const ek_params *p, ek_ctx **out) {
         {(void **)&c->pp.tw, (size_t)p->nx * sizeof(double2)},
         {(void **)&c->pp.piv, (size_t)c->n * c->mp * sizeof(double)},
         {(void **)&c->pp.spec, (size_t)c->n * c->mp * sizeof(double2)},
+        {(void **)&c->kref[0], 3 * (size_t)p->ny * sizeof(float)},
+        {(void **)&c->kref[1], 3 * (size_t)p->ny * sizeof(float)},
     };
     for (auto &a : allocs) {
         e = cudaMalloc(a.ptr, a.bytes);
@@ -397,11 +435,22 @@ int ek_create(const ek_params *p, ek_ctx **out) {
     const double uni[6] = {p->zeta_lo, p->zeta_hi, p->cp_lo, p->cp_hi, p->cn_lo, p->cn_hi};
     for (int k = 0; k < 6; ++k)
         for (int x = 0; x < p->nx; ++x) wall[(size_t)k * p->nx + x] = uni[k];
+    c->kq[0] = ref_exponent(2.0 * std::fabs(p->rho0));
+    c->kq[1] = ref_exponent(2.0 * std::max({std::fabs(p->c0), std::fabs(p->cp_lo), std::fabs(p->cp_hi)}));
+    c->kq[2] = ref_exponent(2.0 * std::max({std::fabs(p->c0), std::fabs(p->cn_lo), std::fabs(p->cn_hi)}));
+    std::vector<float> kref(3 * (size_t)p->ny);
+    const double base[3] = {p->rho0, p->c0, p->c0};
+    for (int sp = 0; sp < 3; ++sp) {
+        const double K = std::nearbyint(base[sp] / 36.0 * std::ldexp(1.0, c->kq[sp]));
+        for (int y = 0; y < p->ny; ++y) kref[(size_t)sp * p->ny + y] = (float)std::ldexp(K, -c->kq[sp]);
+    }
     std::vector<double> piv = make_pivots(*p, c->n, c->mp);
     std::vector<double2> tw = make_twiddles(p->nx);
     c->wall_host = wall;
     e = cudaMemcpyAsync(c->wall, wall.data(), wall.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(c->pp.piv, piv.data(), piv.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->kref[0], kref.data(), kref.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->kref[1], kref.data(), kref.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(c->pp.tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = launch_rates(*p, c->rates_dev, c->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&c->rates, c->rates_dev, sizeof(Rates), cudaMemcpyDeviceToHost, c->stream);
@@ -554,10 +603,13 @@ int ek_init_poisson_boltzmann(ek_ctx *c, int32_t method, int32_t iterations, dou
 int ek_init_equilibrium(ek_ctx *c) {
     if (!c) return fail(EK_ERR_INVALID, "null context");
     const bool ee = c->explicit_e_once || (c->p.flags & EK_FLAG_EXPLICIT_E);
-    if (c->p.storage == EK_STORE_F64)
+    if (c->p.storage == EK_STORE_F64) {
         EK_CUDA(launch_init_f64(c->chan, (double *)c->pops[c->cur], c->fields, ee, c->stream), "init kernel");
-    else
+    } else {
+        int rc = refs_from_fields(c, c->kref[c->kcur]);
+        if (rc != EK_OK) return rc;
         EK_CUDA(launch_init_shifted(c->chan, c->p.storage, c->pops[c->cur], c->fields, ee, c->stream), "init kernel");
+    }
     c->initialised = true;
     c->state_pre = true;
     c->steps = 0;
@@ -571,7 +623,8 @@ int ek_step(ek_ctx *c, int32_t nsteps) {
     const bool every = (c->p.flags & EK_FLAG_MOMENTS_EVERY_STEP) != 0;
     for (int32_t i = 0; i < nsteps; ++i) {
         const bool ee = c->explicit_e_once || (c->p.flags & EK_FLAG_EXPLICIT_E);
-        const bool mom = every || i == nsteps - 1;
+        const bool rebase = shifted(c) && c->rebase_every > 0 && (c->steps + 1) % c->rebase_every == 0;
+        const bool mom = every || i == nsteps - 1 || rebase;
         int rc0 = timed(c, 0, "LBM step kernel", [&] {
             if (c->p.storage == EK_STORE_F64)
                 return launch_step_f64(c->chan, (const double *)c->pops[c->cur], (double *)c->pops[c->cur ^ 1],
@@ -585,8 +638,24 @@ int ek_step(ek_ctx *c, int32_t nsteps) {
         c->explicit_e_once = false;
         int rc = poisson_now(c);
         if (rc != EK_OK) return rc;
+        if (rebase) {
+            rc = rebase_now(c);
+            if (rc != EK_OK) return rc;
+        }
         ++c->steps;
     }
+    return EK_OK;
+}
+
+int ek_rebase(ek_ctx *c) {
+    if (!c) return fail(EK_ERR_INVALID, "null context");
+    if (!shifted(c) || !c->initialised) return EK_OK;
+    return rebase_now(c);
+}
+
+int ek_set_rebase_interval(ek_ctx *c, int32_t steps) {
+    if (!c || steps < 0) return fail(EK_ERR_INVALID, "null context or negative interval");
+    c->rebase_every = steps;
     return EK_OK;
 }
 

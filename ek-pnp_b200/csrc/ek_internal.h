@@ -51,6 +51,11 @@ struct Chan {
     double mob_p, mob_n, f_charge, eps, ext_x, exf;
     Rates r;
     const double *zlo, *zhi, *cplo, *cphi, *cnlo, *cnhi;  // per-x wall values (nx each)
+    // Shifted storage only: per-row reference densities divided by 36, three
+    // rows of ny floats (fluid, c+, c-).  A population of species s stored at
+    // row y holds f - w_i * 36 * kref[s*ny + y]; every kref value is a
+    // multiple of 2^-q, so 36 w_i (kref[y'] - kref[y]) is exact in FP32.
+    const float *kref;
 };
 
 enum Field { F_RHO = 0, F_UX, F_UY, F_CP, F_CN, F_PSI, F_EX, F_EY, F_RHS, F_COUNT };
@@ -74,6 +79,13 @@ cudaError_t launch_step_shifted(const Chan &c, int storage, const void *src, voi
                                 bool first, bool explicit_e, bool moments, cudaStream_t s);
 cudaError_t launch_init_shifted(const Chan &c, int storage, void *pops, const double *fields, bool explicit_e,
                                 cudaStream_t s);
+// Row means of rho, c+, c- rounded to the grid K 2^-q, stored /36 in
+// kout[3*ny] (ek_lbm_f32.cu); q per species.
+cudaError_t launch_row_refs(const Chan &c, const double *fields, int qf, int qp, int qn, float *kout,
+                            cudaStream_t s);
+// Re-express stored shifted populations against a new reference profile.
+cudaError_t launch_rebase(const Chan &c, int storage, void *pops, const float *kold, const float *knew,
+                          cudaStream_t s);
 inline size_t pop_elem_bytes(int storage) { return storage == EK_STORE_F64 ? 8 : (storage == EK_STORE_F32 ? 4 : 2); }
 
 // ---- Poisson (ek_poisson.cu) ----

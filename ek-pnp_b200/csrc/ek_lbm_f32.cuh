@@ -2,9 +2,13 @@
 // populations, FP32 arithmetic).  Included by the single-channel kernels
 // (ek_lbm_f32.cu) and the batched persistent kernel (ek_batch.cu).
 //
-// Storage: d_i = f_i - w_i*R with R = rho0 for the fluid and c0 for both ion
-// species.  Every quantity of the collision is rewritten in deviations so
-// that FP32 keeps the small departures from the reference state:
+// Storage: d_i = f_i - w_i*R with R = R_s(y) a per-row reference density of
+// species s (fluid, c+, c-) at the row where the value is stored.  R_s(y) =
+// 36 K 2^-q for integers K, so the change of frame when a population is pulled
+// from row y' to row y, d += w_i (R_s(y') - R_s(y)) = (16|4|1) (K' - K) 2^-q, is
+// exact in FP32; the profiles follow the fields' row means (set at
+// initialisation, re-based on request).  Every quantity of the collision is
+// rewritten in deviations so that FP32 keeps the small departures:
 //   dens = R + sum_i d_i,  j = sum_i c_i d_i  (sum_i w_i c_i = 0)
 //   deq_i = w_i*(d_dens + dens*A_i),  A_i = cu_i*(1 + cu_i/2) - u^2/(2 cs2)
 //   TRT:  s = (d_i + d_ibar)/2, a = (d_i - d_ibar)/2,
@@ -35,8 +39,11 @@ struct ChanF {
     float rho0, c0;
     float mob_p, mob_n;
     float ms, md;                    // moving top wall terms
+    // FP64 constants of the fluid relaxation + Guo source (see node_shifted)
+    double wpd, wmd, spd, smd, kcud, hinvcs2d, gFd, inv_cs2d, dtd;
     double f_charge, eps, ext_x, exf, dx, dy;
     const double *zlo, *zhi, *cplo, *cphi, *cnlo, *cnhi;
+    const float *kref;               // per-row references / 36 (see Chan::kref)
 };
 
 template <typename S> __device__ __forceinline__ float ld_pop(const S *p);
@@ -69,7 +76,19 @@ __device__ __forceinline__ void pull9s(const S *__restrict__ b, size_t pl, int n
     p[8] = ld_pop<S>(b + 8 * pl + rp + xm);
 }
 
-// Ion anti-bounce-back in deviations: d_ibar = -q_i + 2 w_i (c_wall - c0).
+// Change of frame of pulled populations to the puller's row reference:
+// directions 2, 5, 6 came from row y-1 (dm = kref[y-1] - kref[y]), 4, 7, 8
+// from row y+1 (dp = kref[y+1] - kref[y]); 36 w = 4 (straight), 1 (diagonal).
+__device__ __forceinline__ void reframe(float p[9], float dm, float dp) {
+    p[2] += 4.0f * dm;
+    p[5] += dm;
+    p[6] += dm;
+    p[4] += 4.0f * dp;
+    p[7] += dp;
+    p[8] += dp;
+}
+
+// Ion anti-bounce-back in deviations: d_ibar = -q_i + 2 w_i (c_wall - R).
 __device__ __forceinline__ void ion_wall_dev(const float q[9], float dcw, float p[9]) {
     const float m0 = 2.0f * W0F * dcw, ms = 2.0f * WSF * dcw, md = 2.0f * WDF * dcw;
     p[0] = -q[0] + m0;
@@ -83,54 +102,87 @@ __device__ __forceinline__ void ion_wall_dev(const float q[9], float dcw, float 
     p[6] = -q[8] + md;
 }
 
+// Moments with opposite directions paired first.  In the double layer the
+// y-opposite populations carry large, nearly opposite parts (the force-
+// balanced y-flux); adding those partners first cancels them exactly
+// (Sterbenz), so the small remaining sums round at their own scale.
 __device__ __forceinline__ float sum9f(const float t[9]) {
-    return ((t[0] + t[1]) + (t[2] + t[3])) + ((t[4] + t[5]) + (t[6] + t[7])) + t[8];
+    return (t[0] + (t[1] + t[3])) + ((t[2] + t[4]) + ((t[5] + t[7]) + (t[6] + t[8])));
+}
+__device__ __forceinline__ float momx(const float t[9]) {
+    return (t[1] - t[3]) + ((t[5] + t[8]) - (t[6] + t[7]));
+}
+__device__ __forceinline__ float momy(const float t[9]) {
+    return (t[2] - t[4]) + ((t[5] + t[6]) - (t[7] + t[8]));
 }
 
+// Constants of the collision in compute type T.
+template <typename T> struct CollK {
+    T wp, wm, sp, sm, kcu, hinvcs2, gF, inv_cs2, dt;
+};
+// v/36.  FP64: multiplication by the rounded 1/36 (relative bias 1e-17).
+// FP32 (ion species only): likewise; the resulting 7e-9 bias of the ion
+// equilibrium flux does not accumulate, because the ion flux is not a
+// conserved quantity (the fluid momentum, which is, runs in FP64).
+__device__ __forceinline__ float div36(float v) { return v * (1.0f / 36.0f); }
+__device__ __forceinline__ double div36(double v) { return v * (1.0 / 36.0); }
+
 // TRT of one pair in deviations.  w: lattice weight, cu: (c_i.u)*kcu,
-// base: d_dens - dens*usq (symmetric equilibrium without the cu^2 term).
-__device__ __forceinline__ void trt_pair_dev(float &da, float &db, float w, float dens, float cu, float base,
-                                             float wp, float wm) {
-    const float seq = w * (base + dens * (0.5f * cu * cu));
-    const float aeq = w * dens * cu;
-    const float s = 0.5f * (da + db), a = 0.5f * (da - db);
-    const float ps = wp * (s - seq), pa = wm * (a - aeq);
+// base: d_dens - dens*usq (symmetric equilibrium without the cu^2 term),
+// aeq: antisymmetric equilibrium w*dens*cu (built by the caller, see trt_dev).
+template <typename T>
+__device__ __forceinline__ void trt_pair_dev(T &da, T &db, T w, T dens, T cu, T base, T aeq, T wp, T wm) {
+    const T seq = w * (base + dens * (T(0.5) * cu * cu));
+    const T s = T(0.5) * (da + db), a = T(0.5) * (da - db);
+    const T ps = wp * (s - seq), pa = wm * (a - aeq);
     da = da - ps - pa;
     db = db - ps + pa;
 }
 
 // Full TRT of one species in deviations, in place.  ux, uy: the species'
 // advection velocity; usq_rest: u^2 used by the rest equilibrium.
-__device__ __forceinline__ void trt_dev(float d[9], float ddens, float dens, float ux, float uy, float usq_rest,
-                                        float wp, float wm, const ChanF &k) {
-    const float usq = k.hinvcs2 * (ux * ux + uy * uy);
-    const float base = ddens - dens * usq;
-    const float e0 = W0F * (ddens - dens * (k.hinvcs2 * usq_rest));
+// The antisymmetric equilibria carry the momentum (w- relaxes it to them
+// every step): they are built from the units dens*cu/36 times the exact
+// integers 36 w = 4 or 1, so that their momentum is dens*u up to the rounding
+// of the unit; with weights w rounded to FP32 it would be dens*u*(1+7.4e-9),
+// which the fluid, whose momentum is conserved, would gain step after step.
+template <typename T>
+__device__ __forceinline__ void trt_dev(T d[9], T ddens, T dens, T ux, T uy, T usq_rest, T wp, T wm,
+                                        const CollK<T> &k) {
+    const T w0 = T(4.0 / 9.0), ws = T(1.0 / 9.0), wd = T(1.0 / 36.0);
+    const T usq = k.hinvcs2 * (ux * ux + uy * uy);
+    const T base = ddens - dens * usq;
+    const T e0 = w0 * (ddens - dens * (k.hinvcs2 * usq_rest));
     d[0] = d[0] - wp * (d[0] - e0);
-    const float cx = ux * k.kcu, cy = uy * k.kcu;
-    trt_pair_dev(d[1], d[3], WSF, dens, cx, base, wp, wm);
-    trt_pair_dev(d[2], d[4], WSF, dens, cy, base, wp, wm);
-    trt_pair_dev(d[5], d[7], WDF, dens, cx + cy, base, wp, wm);
-    trt_pair_dev(d[6], d[8], WDF, dens, cy - cx, base, wp, wm);
+    const T cx = ux * k.kcu, cy = uy * k.kcu;
+    const T ax = div36(dens * cx), ay = div36(dens * cy);
+    trt_pair_dev<T>(d[1], d[3], ws, dens, cx, base, T(4) * ax, wp, wm);
+    trt_pair_dev<T>(d[2], d[4], ws, dens, cy, base, T(4) * ay, wp, wm);
+    trt_pair_dev<T>(d[5], d[7], wd, dens, cx + cy, base, ax + ay, wp, wm);
+    trt_pair_dev<T>(d[6], d[8], wd, dens, cy - cx, base, ay - ax, wp, wm);
 }
 
 // Guo source added to post-collision fluid deviations.
-__device__ __forceinline__ void add_guo(float d[9], float ux, float uy, float fx, float fy, const ChanF &k) {
-    const float uF = k.inv_cs2 * (ux * fx + uy * fy);
-    const float cux = ux * k.kcu, cuy = uy * k.kcu;
-    const float cfx = fx * k.gF, cfy = fy * k.gF;
-    const float sp = k.sp * k.dt, sm = k.sm * k.dt;
-    d[0] += sp * (W0F * -uF);
-    // pair (a, abar) with c_a.u -> cu, c_a.F -> cf
-    auto pair = [&](float &da, float &db, float w, float cu, float cf) {
-        const float fp = w * (cu * cf - uF), fm = w * cf;
+template <typename T>
+__device__ __forceinline__ void add_guo(T d[9], T ux, T uy, T fx, T fy, const CollK<T> &k) {
+    const T w0 = T(4.0 / 9.0), ws = T(1.0 / 9.0), wd = T(1.0 / 36.0);
+    const T uF = k.inv_cs2 * (ux * fx + uy * fy);
+    const T cux = ux * k.kcu, cuy = uy * k.kcu;
+    const T cfx = fx * k.gF, cfy = fy * k.gF;
+    const T sp = k.sp * k.dt, sm = k.sm * k.dt;
+    d[0] += sp * (w0 * -uF);
+    // pair (a, abar) with c_a.u -> cu, c_a.F -> cf; the momentum-carrying
+    // part w*cf is built from cf/36 times 36 w = 4 or 1 (see trt_dev)
+    const T gx = div36(cfx), gy = div36(cfy);
+    auto pair = [&](T &da, T &db, T w, T cu, T cf, T fm) {
+        const T fp = w * (cu * cf - uF);
         da += sp * fp + sm * fm;
         db += sp * fp - sm * fm;
     };
-    pair(d[1], d[3], WSF, cux, cfx);
-    pair(d[2], d[4], WSF, cuy, cfy);
-    pair(d[5], d[7], WDF, cux + cuy, cfx + cfy);
-    pair(d[6], d[8], WDF, cuy - cux, cfy - cfx);
+    pair(d[1], d[3], ws, cux, cfx, T(4) * gx);
+    pair(d[2], d[4], ws, cuy, cfy, T(4) * gy);
+    pair(d[5], d[7], wd, cux + cuy, cfx + cfy, gx + gy);
+    pair(d[6], d[8], wd, cuy - cux, cfy - cfx, gy - gx);
 }
 
 __device__ __forceinline__ void efield_at_d(const double *__restrict__ psi, int nxp, int ny, double dx, double dy,
@@ -153,6 +205,10 @@ __device__ __forceinline__ void node_shifted(const ChanF &k, const S *__restrict
     const int xm = x == 0 ? k.nx - 1 : x - 1, xp = x + 1 == k.nx ? 0 : x + 1;
     const int ym = y == 0 ? k.ny - 1 : y - 1, yp = y + 1 == k.ny ? 0 : y + 1;
     const S *sf = src, *sh = src + 9 * pl, *st = src + 18 * pl;
+    const int ny = k.ny;
+    // row references (/36) of the three species at rows y, y-1, y+1
+    const float kf0 = __ldg(k.kref + y), kh0 = __ldg(k.kref + ny + y), kt0 = __ldg(k.kref + 2 * ny + y);
+    const double Rf = 36.0 * kf0, Rh = 36.0 * kh0, Rt = 36.0 * kt0;
 
     float f[9], h[9], t[9];
     if (FIRST) {
@@ -161,19 +217,23 @@ __device__ __forceinline__ void node_shifted(const ChanF &k, const S *__restrict
         own9s<S>(st, pl, o, t);
     } else {
         pull9s<S>(sf, pl, nxp, x, y, xm, xp, ym, yp, f);
+        reframe(f, __ldg(k.kref + ym) - kf0, __ldg(k.kref + yp) - kf0);
         if (lo || hi) {
             float q[9];
             own9s<S>(sh, pl, o, q);
-            ion_wall_dev(q, (float)((lo ? k.cplo[x] : k.cphi[x]) - (double)k.c0), h);
+            ion_wall_dev(q, (float)((lo ? k.cplo[x] : k.cphi[x]) - Rh), h);
             own9s<S>(st, pl, o, q);
-            ion_wall_dev(q, (float)((lo ? k.cnlo[x] : k.cnhi[x]) - (double)k.c0), t);
+            ion_wall_dev(q, (float)((lo ? k.cnlo[x] : k.cnhi[x]) - Rt), t);
         } else {
             pull9s<S>(sh, pl, nxp, x, y, xm, xp, ym, yp, h);
+            reframe(h, __ldg(k.kref + ny + ym) - kh0, __ldg(k.kref + ny + yp) - kh0);
             pull9s<S>(st, pl, nxp, x, y, xm, xp, ym, yp, t);
+            reframe(t, __ldg(k.kref + 2 * ny + ym) - kt0, __ldg(k.kref + 2 * ny + yp) - kt0);
         }
     }
     const float drho = sum9f(f), dcp = sum9f(h), dcn = sum9f(t);
-    const float rho = k.rho0 + drho, cp = k.c0 + dcp, cn = k.c0 + dcn;
+    const float rho = (float)(Rf + (double)drho);
+    const float cp = (float)(Rh + (double)dcp), cn = (float)(Rt + (double)dcn);
     double exd, eyd;
     if (EXPLICIT_E) {
         exd = fields[F_EX * pl + o];
@@ -183,50 +243,55 @@ __device__ __forceinline__ void node_shifted(const ChanF &k, const S *__restrict
     }
     const float Ex = (float)exd, Ey = (float)eyd;
     float fx = 0.0f, fy = 0.0f;
+    const double qnet = (Rh - Rt) + ((double)dcp - (double)dcn);  // c+ - c-
     if (k.flags & EK_FLAG_FORCE) {
-        const double q = k.f_charge * ((double)dcp - (double)dcn);
+        const double q = k.f_charge * qnet;
         fx = (float)(q * (exd + k.ext_x) + k.exf);
         fy = (float)(q * eyd);
     }
-    const float jx = (f[1] + f[5] + f[8]) - (f[3] + f[6] + f[7]);
-    const float jy = (f[2] + f[5] + f[6]) - (f[4] + f[7] + f[8]);
-    float ux = (jx * k.inv_cfl + fx * k.half_dt) / rho;
-    float uy = (jy * k.inv_cfl + fy * k.half_dt) / rho;
+    float ux = (momx(f) * k.inv_cfl + fx * k.half_dt) / rho;
+    float uy = (momy(f) * k.inv_cfl + fy * k.half_dt) / rho;
     if (lo) {
         float m[9];
         const size_t o1 = (size_t)nxp + x;
-        if (FIRST) own9s<S>(sf, pl, o1, m);
-        else pull9s<S>(sf, pl, nxp, x, 1, xm, xp, 0, 2, m);
-        const float rho1 = k.rho0 + sum9f(m);
-        const float jx1 = (m[1] + m[5] + m[8]) - (m[3] + m[6] + m[7]);
-        const float jy1 = (m[2] + m[5] + m[6]) - (m[4] + m[7] + m[8]);
-        ux = -(jx1 * k.inv_cfl + fx * k.half_dt) / rho1;
-        uy = -(jy1 * k.inv_cfl + fy * k.half_dt) / rho1;
+        const float kf1 = __ldg(k.kref + 1);
+        if (FIRST) {
+            own9s<S>(sf, pl, o1, m);
+        } else {
+            pull9s<S>(sf, pl, nxp, x, 1, xm, xp, 0, 2, m);
+            reframe(m, __ldg(k.kref + 0) - kf1, __ldg(k.kref + 2) - kf1);
+        }
+        const float rho1 = (float)(36.0 * kf1 + (double)sum9f(m));
+        ux = -(momx(m) * k.inv_cfl + fx * k.half_dt) / rho1;
+        uy = -(momy(m) * k.inv_cfl + fy * k.half_dt) / rho1;
     }
     if (MOMENTS) {
-        fields[F_RHO * pl + o] = (double)k.rho0 + (double)drho;
+        fields[F_RHO * pl + o] = Rf + (double)drho;
         fields[F_UX * pl + o] = ux;
         fields[F_UY * pl + o] = uy;
-        fields[F_CP * pl + o] = (double)k.c0 + (double)dcp;
-        fields[F_CN * pl + o] = (double)k.c0 + (double)dcn;
+        fields[F_CP * pl + o] = Rh + (double)dcp;
+        fields[F_CN * pl + o] = Rt + (double)dcn;
     }
     if (!lo && !hi) {
-        double v = -k.f_charge * ((double)dcp - (double)dcn) / k.eps;
+        double v = -k.f_charge * qnet / k.eps;
         if (y == 1) v = v - k.zlo[x] / k.dy / k.dy;
         if (y == k.ny - 2) v = v - k.zhi[x] / k.dy / k.dy;
         fields[F_RHS * pl + o] = v;
     }
-    const float usq_f = ux * ux + uy * uy;
+    const float uxf = ux, uyf = uy;
+    const float usq_f = uxf * uxf + uyf * uyf;
+    const CollK<float> kf{k.wp, k.wm, k.sp, k.sm, k.kcu, k.hinvcs2, k.gF, k.inv_cs2, k.dt};
     {
-        const float vx = ux + k.mob_p * Ex, vy = uy + k.mob_p * Ey;
-        trt_dev(h, dcp, cp, vx, vy, vx * vx + vy * vy, k.wcp, k.wcm, k);
+        const float vx = uxf + k.mob_p * Ex, vy = uyf + k.mob_p * Ey;
+        trt_dev<float>(h, dcp, cp, vx, vy, vx * vx + vy * vy, k.wcp, k.wcm, kf);
         S *dh = dst + 9 * pl;
 #pragma unroll
         for (int d = 0; d < 9; ++d) st_pop<S>(dh + d * pl + o, h[d]);
     }
     {
-        const float vx = ux + k.mob_n * Ex, vy = uy + k.mob_n * Ey;
-        trt_dev(t, dcn, cn, vx, vy, (k.flags & EK_FLAG_REST_QUIRK) ? usq_f : vx * vx + vy * vy, k.wtp, k.wtm, k);
+        const float vx = uxf + k.mob_n * Ex, vy = uyf + k.mob_n * Ey;
+        trt_dev<float>(t, dcn, cn, vx, vy, (k.flags & EK_FLAG_REST_QUIRK) ? usq_f : vx * vx + vy * vy, k.wtp,
+                       k.wtm, kf);
         S *dt_ = dst + 18 * pl;
 #pragma unroll
         for (int d = 0; d < 9; ++d) st_pop<S>(dt_ + d * pl + o, t[d]);
@@ -250,10 +315,21 @@ __device__ __forceinline__ void node_shifted(const ChanF &k, const S *__restrict
         st_pop<S>(df + 6 * pl + o, f[8] - k.md);
         return;
     }
-    trt_dev(f, drho, rho, ux, uy, usq_f, k.wp, k.wm, k);
-    if (k.flags & EK_FLAG_FORCE) add_guo(f, ux, uy, fx, fy, k);
+    // Fluid relaxation and Guo source in FP64 on the FP32 moments, rounded
+    // once on the store.  In the double layer the y-force is ~1e3-1e4 x the
+    // x-force and the diagonal populations carry both: FP32 sums such as
+    // g_x + g_y of the diagonal source terms would cost the x-force a relative
+    // 1e-4 of its diagonal share every step (measured: u_x error 6e-5 against
+    // 2e-6 with this form).
+    const CollK<double> kd{k.wpd, k.wmd, k.spd, k.smd, k.kcud, k.hinvcs2d, k.gFd, k.inv_cs2d, k.dtd};
+    double fd[9];
 #pragma unroll
-    for (int d = 0; d < 9; ++d) st_pop<S>(df + d * pl + o, f[d]);
+    for (int q = 0; q < 9; ++q) fd[q] = (double)f[q];
+    const double uxd = ux, uyd = uy;
+    trt_dev<double>(fd, (double)drho, (double)rho, uxd, uyd, uxd * uxd + uyd * uyd, k.wpd, k.wmd, kd);
+    if (k.flags & EK_FLAG_FORCE) add_guo<double>(fd, uxd, uyd, (double)fx, (double)fy, kd);
+#pragma unroll
+    for (int d = 0; d < 9; ++d) st_pop<S>(df + d * pl + o, (float)fd[d]);
 }
 
 // Equilibrium deviations from the fields (pre-collision layout).
@@ -271,25 +347,27 @@ __device__ __forceinline__ void init_node_shifted(const ChanF &k, S *__restrict_
     }
     const float ux = (float)fields[F_UX * pl + o], uy = (float)fields[F_UY * pl + o];
     const float Ex = (float)exd, Ey = (float)eyd;
-    const float dens[3] = {(float)fields[F_RHO * pl + o], (float)fields[F_CP * pl + o], (float)fields[F_CN * pl + o]};
-    const float ref[3] = {k.rho0, k.c0, k.c0};
+    const double densd[3] = {fields[F_RHO * pl + o], fields[F_CP * pl + o], fields[F_CN * pl + o]};
+    const float dens[3] = {(float)densd[0], (float)densd[1], (float)densd[2]};
     const float mob[3] = {0.0f, k.mob_p, k.mob_n};
 #pragma unroll
     for (int s = 0; s < 3; ++s) {
         const float vx = ux + mob[s] * Ex, vy = uy + mob[s] * Ey;
         const float usq = k.hinvcs2 * (vx * vx + vy * vy);
-        const float dd = (float)((double)dens[s] - (double)ref[s]);
+        const float dd = (float)(densd[s] - 36.0 * (double)__ldg(k.kref + s * k.ny + y));
         const float base = dd - dens[s] * usq;
         const float cx = vx * k.kcu, cy = vy * k.kcu;
+        const float ax = div36(dens[s] * cx), ay = div36(dens[s] * cy);
         float e[9];
         e[0] = W0F * base;
         const float cu[4] = {cx, cy, cx + cy, cy - cx};
+        const float an[4] = {4.0f * ax, 4.0f * ay, ax + ay, ay - ax};
         const int ia[4] = {1, 2, 5, 6};
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const float w = q < 2 ? WSF : WDF;
             const float sym = w * (base + dens[s] * 0.5f * cu[q] * cu[q]);
-            const float anti = w * dens[s] * cu[q];
+            const float anti = an[q];
             e[ia[q]] = sym + anti;
             e[oppd(ia[q])] = sym - anti;
         }

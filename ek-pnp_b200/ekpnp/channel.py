@@ -99,6 +99,12 @@ class Channel:
     def step(self, n=1):
         check(lib().ek_step(self._h, int(n)))
 
+    def rebase(self):
+        check(lib().ek_rebase(self._h))
+
+    def set_rebase_interval(self, steps):
+        check(lib().ek_set_rebase_interval(self._h, int(steps)))
+
     def poisson(self):
         check(lib().ek_poisson(self._h))
 

@@ -167,6 +167,15 @@ int ek_init_equilibrium(ek_ctx *ctx);
  * a three-pass Poisson solve. */
 int ek_step(ek_ctx *ctx, int32_t nsteps);
 
+/* Shifted storage (FP32/FP16) keeps each population as a deviation from a
+ * per-row reference density (fluid, c+, c-) set from the fields' row means by
+ * ek_init_equilibrium.  ek_rebase re-derives the references from the moments
+ * of the last step and re-expresses the stored populations against them
+ * (exactly); ek_set_rebase_interval(ctx, n) does that every n steps inside
+ * ek_step (0 = never, the default).  No effect in FP64. */
+int ek_rebase(ek_ctx *ctx);
+int ek_set_rebase_interval(ek_ctx *ctx, int32_t steps);
+
 /* Poisson solve for the current c+, c- moments, then psi and E:
  * fast_Poisson (poisson.cu:180-208) without its per-call cudaMalloc/Free. */
 int ek_poisson(ek_ctx *ctx);
