@@ -195,39 +195,64 @@ __device__ __forceinline__ void efield_at_d(const double *__restrict__ psi, int 
 
 // One node of one step.  src/dst: 27 population planes (species-major);
 // fields: the channel's 9 FP64 field planes.
-template <typename S, bool FIRST, bool EXPLICIT_E, bool MOMENTS>
-__device__ __forceinline__ void node_shifted(const ChanF &k, const S *__restrict__ src, S *__restrict__ dst,
-                                             double *__restrict__ fields, int x, int y) {
+// Raw populations of one node, as stored: FIRST -> the node's own
+// (pre-collision) values; otherwise the fluid pulled from the neighbours and
+// the ions pulled (interior rows) or the node's own values (wall rows).
+template <typename S, bool FIRST>
+__device__ __forceinline__ void gather_global(const ChanF &k, const S *__restrict__ src, int x, int y, float f[9],
+                                              float h[9], float t[9]) {
     const size_t pl = k.plane;
     const int nxp = k.nxp;
     const size_t o = (size_t)y * nxp + x;
-    const bool lo = y == 0, hi = y == k.ny - 1;
+    const bool wall = y == 0 || y == k.ny - 1;
     const int xm = x == 0 ? k.nx - 1 : x - 1, xp = x + 1 == k.nx ? 0 : x + 1;
     const int ym = y == 0 ? k.ny - 1 : y - 1, yp = y + 1 == k.ny ? 0 : y + 1;
     const S *sf = src, *sh = src + 9 * pl, *st = src + 18 * pl;
-    const int ny = k.ny;
-    // row references (/36) of the three species at rows y, y-1, y+1
-    const float kf0 = __ldg(k.kref + y), kh0 = __ldg(k.kref + ny + y), kt0 = __ldg(k.kref + 2 * ny + y);
-    const double Rf = 36.0 * kf0, Rh = 36.0 * kh0, Rt = 36.0 * kt0;
-
-    float f[9], h[9], t[9];
     if (FIRST) {
         own9s<S>(sf, pl, o, f);
         own9s<S>(sh, pl, o, h);
         own9s<S>(st, pl, o, t);
     } else {
         pull9s<S>(sf, pl, nxp, x, y, xm, xp, ym, yp, f);
+        if (wall) {
+            own9s<S>(sh, pl, o, h);
+            own9s<S>(st, pl, o, t);
+        } else {
+            pull9s<S>(sh, pl, nxp, x, y, xm, xp, ym, yp, h);
+            pull9s<S>(st, pl, nxp, x, y, xm, xp, ym, yp, t);
+        }
+    }
+}
+
+// Collision, walls and stores of one node from its raw populations (see
+// gather_global); src is read only for the lower wall's row-1 pull.
+template <typename S, bool FIRST, bool EXPLICIT_E, bool MOMENTS>
+__device__ __forceinline__ void collide_shifted(const ChanF &k, float f[9], float h[9], float t[9],
+                                                const S *__restrict__ src, S *__restrict__ dst,
+                                                double *__restrict__ fields, int x, int y) {
+    const size_t pl = k.plane;
+    const int nxp = k.nxp;
+    const size_t o = (size_t)y * nxp + x;
+    const bool lo = y == 0, hi = y == k.ny - 1;
+    const int xm = x == 0 ? k.nx - 1 : x - 1, xp = x + 1 == k.nx ? 0 : x + 1;
+    const int ym = y == 0 ? k.ny - 1 : y - 1, yp = y + 1 == k.ny ? 0 : y + 1;
+    const S *sf = src;
+    const int ny = k.ny;
+    // row references (/36) of the three species at rows y, y-1, y+1
+    const float kf0 = __ldg(k.kref + y), kh0 = __ldg(k.kref + ny + y), kt0 = __ldg(k.kref + 2 * ny + y);
+    const double Rf = 36.0 * kf0, Rh = 36.0 * kh0, Rt = 36.0 * kt0;
+    if (!FIRST) {
         reframe(f, __ldg(k.kref + ym) - kf0, __ldg(k.kref + yp) - kf0);
         if (lo || hi) {
             float q[9];
-            own9s<S>(sh, pl, o, q);
+#pragma unroll
+            for (int d = 0; d < 9; ++d) q[d] = h[d];
             ion_wall_dev(q, (float)((lo ? k.cplo[x] : k.cphi[x]) - Rh), h);
-            own9s<S>(st, pl, o, q);
+#pragma unroll
+            for (int d = 0; d < 9; ++d) q[d] = t[d];
             ion_wall_dev(q, (float)((lo ? k.cnlo[x] : k.cnhi[x]) - Rt), t);
         } else {
-            pull9s<S>(sh, pl, nxp, x, y, xm, xp, ym, yp, h);
             reframe(h, __ldg(k.kref + ny + ym) - kh0, __ldg(k.kref + ny + yp) - kh0);
-            pull9s<S>(st, pl, nxp, x, y, xm, xp, ym, yp, t);
             reframe(t, __ldg(k.kref + 2 * ny + ym) - kt0, __ldg(k.kref + 2 * ny + yp) - kt0);
         }
     }
@@ -330,6 +355,14 @@ __device__ __forceinline__ void node_shifted(const ChanF &k, const S *__restrict
     if (k.flags & EK_FLAG_FORCE) add_guo<double>(fd, uxd, uyd, (double)fx, (double)fy, kd);
 #pragma unroll
     for (int d = 0; d < 9; ++d) st_pop<S>(df + d * pl + o, (float)fd[d]);
+}
+
+template <typename S, bool FIRST, bool EXPLICIT_E, bool MOMENTS>
+__device__ __forceinline__ void node_shifted(const ChanF &k, const S *__restrict__ src, S *__restrict__ dst,
+                                             double *__restrict__ fields, int x, int y) {
+    float f[9], h[9], t[9];
+    gather_global<S, FIRST>(k, src, x, y, f, h, t);
+    collide_shifted<S, FIRST, EXPLICIT_E, MOMENTS>(k, f, h, t, src, dst, fields, x, y);
 }
 
 // Equilibrium deviations from the fields (pre-collision layout).

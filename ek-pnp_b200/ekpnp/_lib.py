@@ -84,6 +84,7 @@ _SIGS = {
     "ek_launch_count": ([ctypes.c_void_p, _P(ctypes.c_int64)], ctypes.c_int),
     "ek_poisson_noalloc": ([_P(EkParams)] + [ctypes.c_void_p] * 6, ctypes.c_int),
     "ek_rebase": ([ctypes.c_void_p], ctypes.c_int),
+    "ek_set_option": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64], ctypes.c_int),
     "ek_set_rebase_interval": ([ctypes.c_void_p, ctypes.c_int32], ctypes.c_int),
     "ek_init_poisson_boltzmann": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
                                    ctypes.c_double], ctypes.c_int),

@@ -99,6 +99,10 @@ class Channel:
     def step(self, n=1):
         check(lib().ek_step(self._h, int(n)))
 
+    def set_lbm_kernel(self, form):
+        """'auto', 'plain' or 'tma' (shifted storage; both forms are bit-identical)."""
+        check(lib().ek_set_option(self._h, 1, {"auto": 0, "plain": 1, "tma": 2}[form]))
+
     def rebase(self):
         check(lib().ek_rebase(self._h))
 

@@ -176,6 +176,15 @@ int ek_step(ek_ctx *ctx, int32_t nsteps);
 int ek_rebase(ek_ctx *ctx);
 int ek_set_rebase_interval(ek_ctx *ctx, int32_t steps);
 
+/* Tuning options (ek_set_option).  EK_OPT_LBM_KERNEL selects the form of the
+ * shifted-storage LBM kernel: 0 = automatic (currently the plain form, the
+ * faster one on B200), 1 = plain per-node loads, 2 = TMA-fed pipeline
+ * (producer warp + mbarrier ring of tensor copies).  Both forms give
+ * bit-identical results.  Returns EK_ERR_UNSUPPORTED for a form that this
+ * context cannot run. */
+enum { EK_OPT_LBM_KERNEL = 1 };
+int ek_set_option(ek_ctx *ctx, int32_t option, int64_t value);
+
 /* Poisson solve for the current c+, c- moments, then psi and E:
  * fast_Poisson (poisson.cu:180-208) without its per-call cudaMalloc/Free. */
 int ek_poisson(ek_ctx *ctx);
@@ -202,7 +211,9 @@ int ek_residual(ek_ctx *ctx, int32_t interval, double *out5);
 /* Steps taken since ek_create / ek_init_equilibrium. */
 int ek_step_count(const ek_ctx *ctx, int64_t *out);
 
-/* Wait for the context's stream. */
+/* Wait for the context's stream.  Returns EK_ERR_TIMEOUT if a bounded device
+ * wait of a pipelined kernel gave up since the last check (the error word is
+ * then cleared). */
 int ek_sync(ek_ctx *ctx);
 
 /* Device pointers of the field planes (zero-copy readers).  Order: rho, ux,
