@@ -46,46 +46,7 @@ int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
 }  // namespace
 
-struct ek_ctx {
-    ek_params p{};
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-    int nxp = 0, mp = 0, n = 0;
-    size_t plane = 0;
-    void *pops[2] = {nullptr, nullptr};
-    int cur = 0;
-    bool initialised = false;  // populations exist
-    bool state_pre = false;    // pops[cur] holds pre-collision populations in place
-    bool explicit_e_once = false;
-    bool e_stale = false;      // E planes older than psi
-    double *fields = nullptr;
-    double *wall = nullptr;    // 6 x nx
-    std::vector<double> wall_host;  // host copy of the wall profiles
-    double *snap = nullptr;    // residual snapshot, 4 planes
-    double *part = nullptr;    // residual partial sums
-    bool snap_valid = false;
-    float *kref[2] = {nullptr, nullptr};  // shifted storage: row references /36, double-buffered
-    int kcur = 0;
-    int kq[3] = {0, 0, 0};                // binary exponents of the reference grids
-    int32_t rebase_every = 0;
-    CUtensorMap tmaps[2];                 // shifted storage: TMA descriptors of pops[0], pops[1]
-    bool tma_ok = false;
-    int lbm_kernel = 0;                   // EK_OPT_LBM_KERNEL
-    int *err_dev = nullptr;               // set by bounded device waits
-    Rates *rates_dev = nullptr;
-    Rates rates{};
-    PoissonPlan pp{};
-    Chan chan{};
-    int64_t steps = 0;
-    int64_t launches = 0;
-    // profiling
-    bool prof = false;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
-    std::vector<int> ev_phase;
-    size_t ev_used = 0;
-    cudaEvent_t marks[16] = {};
-};
+#include "ek_ctx.h"
 
 namespace {
 
@@ -354,13 +315,39 @@ bool pb_column(int ny, double dy, double g, double a, double zl, double zh, std:
 
 namespace ek {
 void set_last_error(const char *msg) { g_err = msg; }
-}  // namespace ek
+int ctx_fail(int code, const char *msg) { return fail(code, msg); }
+int ctx_refs_from_fields(ek_ctx *c, float *out) { return refs_from_fields(c, out); }
+void ctx_refresh(ek_ctx *c) { refresh_chan(c); }
 
-// ---- residual kernels (ek_residual.cu) ----
-namespace ek {
-cudaError_t launch_residual_f64(const Chan &c, const double *fields, double *snap, double *part,
-                                int nblocks, double *out8, cudaStream_t s);
-int residual_blocks(const Chan &c);
+int ctx_residual_buffers(ek_ctx *c) {
+    if (c->snap) return EK_OK;
+    EK_CUDA(cudaMalloc(&c->snap, 4 * c->plane * sizeof(double)), "residual snapshot");
+    EK_CUDA(cudaMemsetAsync(c->snap, 0, 4 * c->plane * sizeof(double), c->stream), "residual snapshot");
+    EK_CUDA(cudaMalloc(&c->part, (size_t)residual_blocks(c->chan) * 8 * sizeof(double) + 8 * sizeof(double)),
+            "residual partials");
+    return EK_OK;
+}
+
+// out5 = per-field residuals |q - q_snap| / (interval |q|) and their maximum
+// (infinite before the first snapshot).
+int ctx_residual_finish(ek_ctx *c, const double *sums, int32_t interval, double *out5) {
+    for (int k = 0; k < 8; ++k)
+        if (!std::isfinite(sums[k])) return fail(EK_ERR_NAN, "non-finite value in ux, c+, c- or psi");
+    const bool had = c->snap_valid;
+    c->snap_valid = true;
+    const double nn = (double)c->p.nx * (double)c->p.ny;
+    // u_x is normalised by at least the Helmholtz-Smoluchowski speed |eps zeta E/(rho nu)|
+    const double uhs = std::fabs(c->p.eps * c->p.zeta_lo * c->p.ext_x / (c->p.rho0 * c->p.nu));
+    const double floors[4] = {std::max(uhs * std::sqrt(nn), 1e-300), 1e-300, 1e-300, 1e-300};
+    double worst = 0.0;
+    for (int q = 0; q < 4; ++q) {
+        const double norm = std::max(std::sqrt(sums[4 + q]), floors[q]);
+        out5[q] = had ? std::sqrt(sums[q]) / ((double)interval * norm) : INFINITY;
+        worst = std::max(worst, out5[q]);
+    }
+    out5[4] = worst;
+    return EK_OK;
+}
 }  // namespace ek
 
 extern "C" {
@@ -733,12 +720,8 @@ int ek_get_fields_device(ek_ctx *c, double *rho, double *ux, double *uy, double 
 
 int ek_residual(ek_ctx *c, int32_t interval, double *out5) {
     if (!c || !out5 || interval <= 0) return fail(EK_ERR_INVALID, "bad residual arguments");
-    if (!c->snap) {
-        EK_CUDA(cudaMalloc(&c->snap, 4 * c->plane * sizeof(double)), "residual snapshot");
-        EK_CUDA(cudaMemsetAsync(c->snap, 0, 4 * c->plane * sizeof(double), c->stream), "residual snapshot");
-        EK_CUDA(cudaMalloc(&c->part, (size_t)residual_blocks(c->chan) * 8 * sizeof(double) + 8 * sizeof(double)),
-                "residual partials");
-    }
+    int rc = ek::ctx_residual_buffers(c);
+    if (rc != EK_OK) return rc;
     double sums[8];
     const int nb = residual_blocks(c->chan);
     EK_CUDA(launch_residual_f64(c->chan, c->fields, c->snap, c->part, nb, c->part + (size_t)nb * 8, c->stream),
@@ -746,22 +729,7 @@ int ek_residual(ek_ctx *c, int32_t interval, double *out5) {
     EK_CUDA(cudaMemcpyAsync(sums, c->part + (size_t)nb * 8, sizeof(sums), cudaMemcpyDeviceToHost, c->stream),
             "residual copy");
     EK_CUDA(cudaStreamSynchronize(c->stream), "residual sync");
-    for (double v : sums)
-        if (!std::isfinite(v)) return fail(EK_ERR_NAN, "non-finite value in ux, c+, c- or psi");
-    const bool had = c->snap_valid;
-    c->snap_valid = true;
-    const double nn = (double)c->p.nx * (double)c->p.ny;
-    // u_x is normalised by at least the Helmholtz-Smoluchowski speed |eps zeta E/(rho nu)|
-    const double uhs = std::fabs(c->p.eps * c->p.zeta_lo * c->p.ext_x / (c->p.rho0 * c->p.nu));
-    const double floors[4] = {std::max(uhs * std::sqrt(nn), 1e-300), 1e-300, 1e-300, 1e-300};
-    double worst = 0.0;
-    for (int q = 0; q < 4; ++q) {
-        const double norm = std::max(std::sqrt(sums[4 + q]), floors[q]);
-        out5[q] = had ? std::sqrt(sums[q]) / ((double)interval * norm) : INFINITY;
-        worst = std::max(worst, out5[q]);
-    }
-    out5[4] = worst;
-    return EK_OK;
+    return ek::ctx_residual_finish(c, sums, interval, out5);
 }
 
 int ek_step_count(const ek_ctx *c, int64_t *out) {

@@ -108,6 +108,23 @@ cudaError_t poisson_pass_f64(int pass, const PoissonPlan &pp, const Chan &c, dou
 cudaError_t poisson_pass_f64_at(int pass, const PoissonPlan &pp, const Chan &c, const double *rhs, double *psi,
                                 cudaStream_t s);
 size_t poisson_smem_bytes_f64(int nx);
+// Batched Poisson passes over many channels (ek_batch.cu builds the items):
+// pass 0/2 items int2 {channel, first row pair} (256-thread blocks, each
+// 256/(nx/16) row pairs; power-of-two nx from 16 to 4096); pass 1 items
+// int3 {channel, first mode, modes per block}.
+cudaError_t batch_poisson(int pass, const PoissonPlan *plans, const Chan *chans, double *const *fields,
+                          const void *items, int nitems, cudaStream_t s);
+int poisson_tridiag_modes(int n);
+// Steady-state residual sums (ek_residual.cu): per channel 8 FP64 sums,
+// (q - q_snap)^2 then q^2 for q in (ux, c+, c-, psi); the snapshot is updated.
+cudaError_t launch_residual_f64(const Chan &c, const double *fields, double *snap, double *part,
+                                int nblocks, double *out8, cudaStream_t s);
+int residual_blocks(const Chan &c);
+// Many channels: items int4 {channel, block, blocks of the channel, first
+// partial}, ranges int2 {first partial, blocks} per channel, out8 8 per channel.
+cudaError_t launch_batch_residual(const Chan *chans, double *const *fields, double *const *snaps, const int4 *items,
+                                  int nitems, const int2 *ranges, int nch, double *part, double *out8,
+                                  cudaStream_t s);
 // Record an error message for ek_last_error() (ek_api.cu).
 void set_last_error(const char *msg);
 cudaError_t poisson_set_smem_limits();

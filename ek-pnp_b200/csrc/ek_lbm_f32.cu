@@ -64,12 +64,12 @@ namespace {
 
 constexpr int TPB = 128;
 
-template <typename S, bool FIRST, bool EE, bool MOM>
+template <typename S, bool FIRST, bool EE>
 __global__ void __launch_bounds__(TPB)
-step_shifted(const ChanF k, const S *__restrict__ src, S *__restrict__ dst, double *__restrict__ fields) {
+step_shifted(const ChanF k, const S *__restrict__ src, S *__restrict__ dst, double *__restrict__ fields, bool mom) {
     const int x = blockIdx.x * TPB + threadIdx.x;
     if (x >= k.nx) return;
-    node_shifted<S, FIRST, EE, MOM>(k, src, dst, fields, x, blockIdx.y);
+    node_shifted<S, FIRST, EE>(k, src, dst, fields, x, blockIdx.y, mom);
 }
 
 template <typename S>
@@ -86,64 +86,28 @@ cudaError_t step_typed(const ChanF &k, const void *src, void *dst, double *field
     const dim3 g((k.nx + TPB - 1) / TPB, k.ny);
     const S *a = (const S *)src;
     S *b = (S *)dst;
-#define EK_SS(F, E, M) step_shifted<S, F, E, M><<<g, TPB, 0, s>>>(k, a, b, fields)
-    switch ((first ? 4 : 0) | (ee ? 2 : 0) | (mom ? 1 : 0)) {
-        case 0: EK_SS(false, false, false); break;
-        case 1: EK_SS(false, false, true); break;
-        case 2: EK_SS(false, true, false); break;
-        case 3: EK_SS(false, true, true); break;
-        case 4: EK_SS(true, false, false); break;
-        case 5: EK_SS(true, false, true); break;
-        case 6: EK_SS(true, true, false); break;
-        default: EK_SS(true, true, true); break;
+    if (first) {
+        if (ee) step_shifted<S, true, true><<<g, TPB, 0, s>>>(k, a, b, fields, mom);
+        else step_shifted<S, true, false><<<g, TPB, 0, s>>>(k, a, b, fields, mom);
+    } else {
+        if (ee) step_shifted<S, false, true><<<g, TPB, 0, s>>>(k, a, b, fields, mom);
+        else step_shifted<S, false, false><<<g, TPB, 0, s>>>(k, a, b, fields, mom);
     }
-#undef EK_SS
     return cudaGetLastError();
 }
 
-// Row means of rho, c+, c- rounded to the reference grid K 2^-q (stored /36):
-// one block per row, FP64 sums.
 __global__ void __launch_bounds__(256) row_refs(const Chan c, const double *__restrict__ fields, int qf, int qp,
                                                 int qn, float *__restrict__ kout) {
-    const int y = blockIdx.x;
-    double acc[3] = {0.0, 0.0, 0.0};
-    const size_t r = (size_t)y * c.nxp;
-    for (int x = threadIdx.x; x < c.nx; x += blockDim.x) {
-        acc[0] += fields[F_RHO * c.plane + r + x];
-        acc[1] += fields[F_CP * c.plane + r + x];
-        acc[2] += fields[F_CN * c.plane + r + x];
-    }
-    __shared__ double red[8][3];
-#pragma unroll
-    for (int s = 0; s < 3; ++s) {
-        double v = acc[s];
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][s] = v;
-    }
-    __syncthreads();
-    if (threadIdx.x < 3) {
-        double v = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[w][threadIdx.x];
-        const int q = threadIdx.x == 0 ? qf : (threadIdx.x == 1 ? qp : qn);
-        const double mean = v / (double)c.nx;
-        const double K = rint(mean / 36.0 * ldexp(1.0, q));
-        kout[threadIdx.x * c.ny + y] = (float)ldexp(K, -q);
-    }
+    row_refs_dev(c.nx, c.nxp, c.ny, c.plane, fields, qf, qp, qn, kout, blockIdx.x);
 }
 
-// d += 36 w_d (kold - knew) for every stored value (exact in FP32).
 template <typename S>
 __global__ void __launch_bounds__(TPB) rebase_pops(const Chan c, S *__restrict__ pops, const float *__restrict__ kold,
                                                    const float *__restrict__ knew) {
     const int x = blockIdx.x * TPB + threadIdx.x;
     const int y = blockIdx.y, plane = blockIdx.z;
     if (x >= c.nx) return;
-    const int s = plane / 9, d = plane - 9 * s;
-    const float wint = d == 0 ? 16.0f : (d < 5 ? 4.0f : 1.0f);
-    const float corr = wint * (kold[s * c.ny + y] - knew[s * c.ny + y]);
-    S *p = pops + (size_t)plane * c.plane + (size_t)y * c.nxp + x;
-    st_pop<S>(p, ld_pop<S>(p) + corr);
+    rebase_dev<S>(pops + (size_t)plane * c.plane + (size_t)y * c.nxp + x, plane, c.ny, y, kold, knew);
 }
 
 }  // namespace

@@ -226,10 +226,15 @@ __device__ __forceinline__ void gather_global(const ChanF &k, const S *__restric
 
 // Collision, walls and stores of one node from its raw populations (see
 // gather_global); src is read only for the lower wall's row-1 pull.
-template <typename S, bool FIRST, bool EXPLICIT_E, bool MOMENTS>
+// `moments` is a run-time flag on purpose: as a template parameter it gave
+// two instantiations that the compiler fused into multiply-adds differently,
+// so a step that wrote the moments could round differently from one that
+// did not.  One body with predicated stores keeps every step's arithmetic
+// independent of how the steps are split into calls.
+template <typename S, bool FIRST, bool EXPLICIT_E>
 __device__ __forceinline__ void collide_shifted(const ChanF &k, float f[9], float h[9], float t[9],
                                                 const S *__restrict__ src, S *__restrict__ dst,
-                                                double *__restrict__ fields, int x, int y) {
+                                                double *__restrict__ fields, int x, int y, bool moments) {
     const size_t pl = k.plane;
     const int nxp = k.nxp;
     const size_t o = (size_t)y * nxp + x;
@@ -290,7 +295,7 @@ __device__ __forceinline__ void collide_shifted(const ChanF &k, float f[9], floa
         ux = -(momx(m) * k.inv_cfl + fx * k.half_dt) / rho1;
         uy = -(momy(m) * k.inv_cfl + fy * k.half_dt) / rho1;
     }
-    if (MOMENTS) {
+    if (moments) {
         fields[F_RHO * pl + o] = Rf + (double)drho;
         fields[F_UX * pl + o] = ux;
         fields[F_UY * pl + o] = uy;
@@ -357,12 +362,12 @@ __device__ __forceinline__ void collide_shifted(const ChanF &k, float f[9], floa
     for (int d = 0; d < 9; ++d) st_pop<S>(df + d * pl + o, (float)fd[d]);
 }
 
-template <typename S, bool FIRST, bool EXPLICIT_E, bool MOMENTS>
+template <typename S, bool FIRST, bool EXPLICIT_E>
 __device__ __forceinline__ void node_shifted(const ChanF &k, const S *__restrict__ src, S *__restrict__ dst,
-                                             double *__restrict__ fields, int x, int y) {
+                                             double *__restrict__ fields, int x, int y, bool moments) {
     float f[9], h[9], t[9];
     gather_global<S, FIRST>(k, src, x, y, f, h, t);
-    collide_shifted<S, FIRST, EXPLICIT_E, MOMENTS>(k, f, h, t, src, dst, fields, x, y);
+    collide_shifted<S, FIRST, EXPLICIT_E>(k, f, h, t, src, dst, fields, x, y, moments);
 }
 
 // Equilibrium deviations from the fields (pre-collision layout).
@@ -407,6 +412,47 @@ __device__ __forceinline__ void init_node_shifted(const ChanF &k, S *__restrict_
 #pragma unroll
         for (int d = 0; d < 9; ++d) st_pop<S>(pops + (s * 9 + d) * pl + o, e[d]);
     }
+}
+
+// Row y's means of rho, c+, c- rounded to the reference grids K 2^-q (stored
+// /36), FP64 sums; a block of 256 threads per row, kout[s*ny + y].
+__device__ __forceinline__ void row_refs_dev(int nx, int nxp, int ny, size_t plane, const double *__restrict__ fields,
+                                             int qf, int qp, int qn, float *__restrict__ kout, int y) {
+    double acc[3] = {0.0, 0.0, 0.0};
+    const size_t r = (size_t)y * nxp;
+    for (int x = threadIdx.x; x < nx; x += blockDim.x) {
+        acc[0] += fields[F_RHO * plane + r + x];
+        acc[1] += fields[F_CP * plane + r + x];
+        acc[2] += fields[F_CN * plane + r + x];
+    }
+    __shared__ double red[8][3];
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+        double v = acc[s];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][s] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double v = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[w][threadIdx.x];
+        const int q = threadIdx.x == 0 ? qf : (threadIdx.x == 1 ? qp : qn);
+        const double mean = v / (double)nx;
+        const double K = rint(mean / 36.0 * ldexp(1.0, q));
+        kout[threadIdx.x * ny + y] = (float)ldexp(K, -q);
+    }
+}
+
+// Re-basing of one stored value of plane (species s, direction d) at row y:
+// d += 36 w_d (kold - knew), exact in FP32.
+template <typename S>
+__device__ __forceinline__ void rebase_dev(S *p, int plane_idx, int ny, int y, const float *__restrict__ kold,
+                                           const float *__restrict__ knew) {
+    const int s = plane_idx / 9, d = plane_idx - 9 * s;
+    const float wint = d == 0 ? 16.0f : (d < 5 ? 4.0f : 1.0f);
+    const float corr = wint * (kold[s * ny + y] - knew[s * ny + y]);
+    st_pop<S>(p, ld_pop<S>(p) + corr);
 }
 
 ChanF make_chanf(const Chan &c);

@@ -94,10 +94,10 @@ template <typename S> __device__ __forceinline__ float ld_smem(const S *p);
 template <> __device__ __forceinline__ float ld_smem<float>(const float *p) { return *p; }
 template <> __device__ __forceinline__ float ld_smem<__half>(const __half *p) { return __half2float(*p); }
 
-template <typename S, bool FIRST, bool EE, bool MOM>
+template <typename S, bool FIRST, bool EE>
 __global__ void __launch_bounds__(NTHREADS)
 step_tma(const __grid_constant__ CUtensorMap tsrc, const ChanF k, const S *__restrict__ src, S *__restrict__ dst,
-         double *__restrict__ fields, int *__restrict__ err) {
+         double *__restrict__ fields, int *__restrict__ err, bool mom) {
     using G = Geom<S>;
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *full = (uint64_t *)(smem + NSTAGE * G::STAGE_BYTES);
@@ -173,7 +173,7 @@ step_tma(const __grid_constant__ CUtensorMap tsrc, const ChanF k, const S *__res
                     v[plane] = ld_pop<S>(src + plane * pl + (size_t)row * k.nxp + xs);
                 }
             }
-            collide_shifted<S, FIRST, EE, MOM>(k, v, v + 9, v + 18, src, dst, fields, x, y);
+            collide_shifted<S, FIRST, EE>(k, v, v + 9, v + 18, src, dst, fields, x, y, mom);
         }
     }
 }
@@ -196,16 +196,13 @@ cudaError_t launch_typed(const CUtensorMap &map, const ChanF &k, const void *src
     const S *a = (const S *)src;
     S *b = (S *)dst;
     const int smem = Geom<S>::SMEM_BYTES;
-#define EK_TMA(F, E, M) step_tma<S, F, E, M><<<grid, NTHREADS, smem, s>>>(map, k, a, b, fields, err)
-    switch ((first ? 4 : 0) | (ee ? 2 : 0) | (mom ? 1 : 0)) {
-        case 0: EK_TMA(false, false, false); break;
-        case 1: EK_TMA(false, false, true); break;
-        case 2: EK_TMA(false, true, false); break;
-        case 3: EK_TMA(false, true, true); break;
-        case 4: EK_TMA(true, false, false); break;
-        case 5: EK_TMA(true, false, true); break;
-        case 6: EK_TMA(true, true, false); break;
-        default: EK_TMA(true, true, true); break;
+#define EK_TMA(F, E) step_tma<S, F, E><<<grid, NTHREADS, smem, s>>>(map, k, a, b, fields, err, mom)
+    if (first) {
+        if (ee) EK_TMA(true, true);
+        else EK_TMA(true, false);
+    } else {
+        if (ee) EK_TMA(false, true);
+        else EK_TMA(false, false);
     }
 #undef EK_TMA
     return cudaGetLastError();
@@ -213,10 +210,8 @@ cudaError_t launch_typed(const CUtensorMap &map, const ChanF &k, const void *src
 
 template <typename S> cudaError_t set_attrs() {
     const void *fns[] = {
-        (const void *)step_tma<S, false, false, false>, (const void *)step_tma<S, false, false, true>,
-        (const void *)step_tma<S, false, true, false>,  (const void *)step_tma<S, false, true, true>,
-        (const void *)step_tma<S, true, false, false>,  (const void *)step_tma<S, true, false, true>,
-        (const void *)step_tma<S, true, true, false>,   (const void *)step_tma<S, true, true, true>};
+        (const void *)step_tma<S, false, false>, (const void *)step_tma<S, false, true>,
+        (const void *)step_tma<S, true, false>, (const void *)step_tma<S, true, true>};
     for (const void *f : fns) {
         cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, Geom<S>::SMEM_BYTES);
         if (e != cudaSuccess) return e;
@@ -256,9 +251,9 @@ cudaError_t launch_step_tma(const Chan &c, int storage, const void *map, const v
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const bool half = storage == EK_STORE_F16;
-    cudaError_t e = half ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step_tma<__half, false, false, false>,
+    cudaError_t e = half ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step_tma<__half, false, false>,
                                                                        NTHREADS, Geom<__half>::SMEM_BYTES)
-                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step_tma<float, false, false, false>,
+                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step_tma<float, false, false>,
                                                                        NTHREADS, Geom<float>::SMEM_BYTES);
     if (e != cudaSuccess) return e;
     const int ntiles = ((c.nx + TX - 1) / TX) * c.ny;

@@ -291,13 +291,11 @@ __device__ void reg_fft(double2 *s, int k, int T, int t, const double2 *__restri
 // Pass A, radix-16 form: row pairs (2p+1, 2p+2) of the right-hand side ->
 // spectra.  One block holds BLOCK/T row pairs.
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK, 512 / BLOCK)
-fwd_rows_r16(const PoissonPlan pp, const double *__restrict__ rhs, int nxp) {
-    extern __shared__ double2 sm[];
+__device__ __forceinline__ void fwd_rows_r16_dev(const PoissonPlan &pp, const double *__restrict__ rhs, int nxp,
+                                                 int pair_base, double2 *sm) {
     const int N = pp.nx, k = pp.log2nx, T = N >> 4;
-    const int per = BLOCK / T;
     const int p = threadIdx.x / T, t = threadIdx.x - p * T;
-    const int pair = blockIdx.x * per + p;
+    const int pair = pair_base + p;
     double2 *s = sm + p * N;
     const int j0 = 2 * pair, j1 = j0 + 1;
     const bool live = j0 < pp.n, two = j1 < pp.n;
@@ -315,15 +313,22 @@ fwd_rows_r16(const PoissonPlan pp, const double *__restrict__ rhs, int nxp) {
     }
 }
 
-// Pass C, radix-16 form: spectra -> psi rows; block 0 also writes the walls.
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 512 / BLOCK)
-inv_rows_r16(const PoissonPlan pp, const Chan c, double *__restrict__ psi) {
+fwd_rows_r16(const PoissonPlan pp, const double *__restrict__ rhs, int nxp) {
     extern __shared__ double2 sm[];
+    fwd_rows_r16_dev<BLOCK>(pp, rhs, nxp, blockIdx.x * (BLOCK / (pp.nx >> 4)), sm);
+}
+
+// Pass C, radix-16 form: spectra -> psi rows; the block holding row pair 0
+// also writes the walls.
+template <int BLOCK>
+__device__ __forceinline__ void inv_rows_r16_dev(const PoissonPlan &pp, int nxp, int ny, const double *zlo,
+                                                 const double *zhi, double *__restrict__ psi, int pair_base,
+                                                 double2 *sm) {
     const int N = pp.nx, k = pp.log2nx, T = N >> 4;
-    const int per = BLOCK / T;
     const int p = threadIdx.x / T, t = threadIdx.x - p * T;
-    const int pair = blockIdx.x * per + p;
+    const int pair = pair_base + p;
     double2 *s = sm + p * N;
     const int j0 = 2 * pair, j1 = j0 + 1;
     const bool live = j0 < pp.n, two = j1 < pp.n;
@@ -338,20 +343,27 @@ inv_rows_r16(const PoissonPlan pp, const Chan c, double *__restrict__ psi) {
     reg_fft<true>(s, k, T, t, pp.tw);
     const double inv = 1.0 / (double)N;
     if (live) {
-        double *p0 = psi + (size_t)(j0 + 1) * c.nxp, *p1 = psi + (size_t)(j1 + 1) * c.nxp;
+        double *p0 = psi + (size_t)(j0 + 1) * nxp, *p1 = psi + (size_t)(j1 + 1) * nxp;
         for (int x = t; x < N; x += T) {
             const double2 z = s[swz(x, k)];
             p0[x] = z.x * inv;
             if (two) p1[x] = z.y * inv;
         }
     }
-    if (blockIdx.x == 0) {
-        double *lo = psi, *hi = psi + (size_t)(c.ny - 1) * c.nxp;
+    if (pair_base == 0) {
+        double *lo = psi, *hi = psi + (size_t)(ny - 1) * nxp;
         for (int x = threadIdx.x; x < N; x += BLOCK) {
-            lo[x] = c.zlo[x];
-            hi[x] = c.zhi[x];
+            lo[x] = zlo[x];
+            hi[x] = zhi[x];
         }
     }
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 512 / BLOCK)
+inv_rows_r16(const PoissonPlan pp, const Chan c, double *__restrict__ psi) {
+    extern __shared__ double2 sm[];
+    inv_rows_r16_dev<BLOCK>(pp, c.nxp, c.ny, c.zlo, c.zhi, psi, blockIdx.x * (BLOCK / (pp.nx >> 4)), sm);
 }
 
 // ---- pass B, partitioned Thomas solve ------------------------------------
@@ -368,14 +380,19 @@ inv_rows_r16(const PoissonPlan pp, const Chan c, double *__restrict__ psi) {
 constexpr int TB_THREADS = 512;
 constexpr int TB_L = 16;
 
-__global__ void __launch_bounds__(TB_THREADS) tridiag_part(const PoissonPlan pp, int M) {
-    __shared__ double2 ends[TB_THREADS];
-    __shared__ double mults[TB_THREADS];
-    __shared__ double2 carry[TB_THREADS];
+struct TridiagShared {
+    double2 ends[TB_THREADS];
+    double mults[TB_THREADS];
+    double2 carry[TB_THREADS];
+};
+
+__device__ __forceinline__ void tridiag_part_dev(const PoissonPlan &pp, int M, int m_base, TridiagShared &sh) {
+    double2 *ends = sh.ends, *carry = sh.carry;
+    double *mults = sh.mults;
     const int n = pp.n, mlast = pp.nx / 2;
     const size_t mp = pp.mp;
     const int tid = threadIdx.x, mode = tid % M, seg = tid / M, S = TB_THREADS / M;
-    const int m = blockIdx.x * M + mode;
+    const int m = m_base + mode;
     const bool mvalid = m <= mlast;
     const int L = (n + S - 1) / S, ja = seg * L, cnt = max(0, min(n, ja + L) - ja);
     double c[TB_L];
@@ -459,6 +476,42 @@ __global__ void __launch_bounds__(TB_THREADS) tridiag_part(const PoissonPlan pp,
     }
 }
 
+__global__ void __launch_bounds__(TB_THREADS) tridiag_part(const PoissonPlan pp, int M) {
+    __shared__ TridiagShared sh;
+    tridiag_part_dev(pp, M, blockIdx.x * M, sh);
+}
+
+// ---- batched passes: one launch for many channels -------------------------
+// A block's work item names its channel and its first row pair (passes A,
+// C) or first x-mode (pass B); the channel's plan comes from a device table.
+__global__ void __launch_bounds__(256, 2)
+batch_fwd_rows(const PoissonPlan *__restrict__ plans, const Chan *__restrict__ chans,
+               double *const *__restrict__ fields, const int2 *__restrict__ items) {
+    extern __shared__ double2 sm[];
+    const int2 it = items[blockIdx.x];
+    const PoissonPlan pp = plans[it.x];
+    const Chan &c = chans[it.x];
+    fwd_rows_r16_dev<256>(pp, fields[it.x] + F_RHS * c.plane, c.nxp, it.y, sm);
+}
+
+__global__ void __launch_bounds__(256, 2)
+batch_inv_rows(const PoissonPlan *__restrict__ plans, const Chan *__restrict__ chans,
+               double *const *__restrict__ fields, const int2 *__restrict__ items) {
+    extern __shared__ double2 sm[];
+    const int2 it = items[blockIdx.x];
+    const PoissonPlan pp = plans[it.x];
+    const Chan &c = chans[it.x];
+    inv_rows_r16_dev<256>(pp, c.nxp, c.ny, c.zlo, c.zhi, fields[it.x] + F_PSI * c.plane, it.y, sm);
+}
+
+__global__ void __launch_bounds__(TB_THREADS)
+batch_tridiag(const PoissonPlan *__restrict__ plans, const int3 *__restrict__ items) {
+    __shared__ TridiagShared sh;
+    const int3 it = items[blockIdx.x];
+    const PoissonPlan pp = plans[it.x];
+    tridiag_part_dev(pp, it.z, it.y, sh);
+}
+
 // Modes per block of tridiag_part for n rows, so that every segment has at
 // most TB_L rows (0: too tall, use the one-thread-per-mode `tridiag`).
 int tridiag_modes(int n) {
@@ -518,10 +571,25 @@ cudaError_t poisson_pass_f64_at(int pass, const PoissonPlan &pp, const Chan &c, 
     return cudaGetLastError();
 }
 
+int poisson_tridiag_modes(int n) { return tridiag_modes(n); }
+
+cudaError_t batch_poisson(int pass, const PoissonPlan *plans, const Chan *chans, double *const *fields,
+                          const void *items, int nitems, cudaStream_t s) {
+    if (nitems <= 0) return cudaSuccess;
+    if (pass == 0)
+        batch_fwd_rows<<<nitems, 256, 65536, s>>>(plans, chans, fields, (const int2 *)items);
+    else if (pass == 1)
+        batch_tridiag<<<nitems, TB_THREADS, 0, s>>>(plans, (const int3 *)items);
+    else
+        batch_inv_rows<<<nitems, 256, 65536, s>>>(plans, chans, fields, (const int2 *)items);
+    return cudaGetLastError();
+}
+
 cudaError_t poisson_set_smem_limits() {
     const void *fns[] = {(const void *)fwd_rows, (const void *)inv_rows, (const void *)fwd_rows_r16<256>,
                          (const void *)inv_rows_r16<256>, (const void *)fwd_rows_r16<512>,
-                         (const void *)inv_rows_r16<512>};
+                         (const void *)inv_rows_r16<512>, (const void *)batch_fwd_rows,
+                         (const void *)batch_inv_rows};
     for (const void *f : fns) {
         cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if (e == cudaSuccess)

@@ -19,12 +19,13 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-__global__ void __launch_bounds__(RTPB)
-residual_partials(const Chan c, const double *__restrict__ fields, double *__restrict__ snap,
-                  double *__restrict__ part) {
+// Partial sums of block `blk` of `nblocks` over one channel's nodes.
+__device__ __forceinline__ void residual_partials_dev(const Chan &c, const double *__restrict__ fields,
+                                                      double *__restrict__ snap, double *__restrict__ part, int blk,
+                                                      int nblocks) {
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     const long long nn = (long long)c.nx * c.ny;
-    for (long long i = (long long)blockIdx.x * RTPB + threadIdx.x; i < nn; i += (long long)gridDim.x * RTPB) {
+    for (long long i = (long long)blk * RTPB + threadIdx.x; i < nn; i += (long long)nblocks * RTPB) {
         const int y = (int)(i / c.nx), x = (int)(i - (long long)y * c.nx);
         const size_t o = (size_t)y * c.nxp + x;
 #pragma unroll
@@ -47,8 +48,34 @@ residual_partials(const Chan c, const double *__restrict__ fields, double *__res
     if (threadIdx.x < 8) {
         double s = 0.0;
         for (int w = 0; w < RTPB / 32; ++w) s += red[w][threadIdx.x];
-        part[(size_t)blockIdx.x * 8 + threadIdx.x] = s;
+        part[(size_t)blk * 8 + threadIdx.x] = s;
     }
+}
+
+__global__ void __launch_bounds__(RTPB)
+residual_partials(const Chan c, const double *__restrict__ fields, double *__restrict__ snap,
+                  double *__restrict__ part) {
+    residual_partials_dev(c, fields, snap, part, blockIdx.x, gridDim.x);
+}
+
+// Many channels: item {channel, block, blocks of the channel, first partial}.
+__global__ void __launch_bounds__(RTPB)
+batch_residual_partials(const Chan *__restrict__ chans, double *const *__restrict__ fields,
+                        double *const *__restrict__ snaps, const int4 *__restrict__ items, double *__restrict__ part) {
+    const int4 it = items[blockIdx.x];
+    residual_partials_dev(chans[it.x], fields[it.x], snaps[it.x], part + (size_t)it.w * 8, it.y, it.z);
+}
+
+// One warp per channel: lanes 0..7 sum their column of the channel's
+// partials in block order (the order of residual_final).
+__global__ void batch_residual_final(const int2 *__restrict__ ranges, int nch, const double *__restrict__ part,
+                                     double *__restrict__ out8) {
+    const int ch = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (ch >= nch || lane >= 8) return;
+    const int2 r = ranges[ch];  // {first partial, blocks}
+    double s = 0.0;
+    for (int b = 0; b < r.y; ++b) s += part[(size_t)(r.x + b) * 8 + lane];
+    out8[(size_t)ch * 8 + lane] = s;
 }
 
 __global__ void residual_final(const double *__restrict__ part, int nblocks, double *__restrict__ out8) {
@@ -72,6 +99,14 @@ cudaError_t launch_residual_f64(const Chan &c, const double *fields, double *sna
                                 int nblocks, double *out8, cudaStream_t s) {
     residual_partials<<<nblocks, RTPB, 0, s>>>(c, fields, snap, part);
     residual_final<<<1, 32, 0, s>>>(part, nblocks, out8);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_residual(const Chan *chans, double *const *fields, double *const *snaps, const int4 *items,
+                                  int nitems, const int2 *ranges, int nch, double *part, double *out8,
+                                  cudaStream_t s) {
+    batch_residual_partials<<<nitems, RTPB, 0, s>>>(chans, fields, snaps, items, part);
+    batch_residual_final<<<(nch + 7) / 8, 256, 0, s>>>(ranges, nch, part, out8);
     return cudaGetLastError();
 }
 

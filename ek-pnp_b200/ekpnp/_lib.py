@@ -88,6 +88,21 @@ _SIGS = {
     "ek_set_rebase_interval": ([ctypes.c_void_p, ctypes.c_int32], ctypes.c_int),
     "ek_init_poisson_boltzmann": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
                                    ctypes.c_double], ctypes.c_int),
+    "ek_batch_create": ([ctypes.c_void_p, ctypes.c_int32, _P(ctypes.c_void_p)], ctypes.c_int),
+    "ek_batch_destroy": ([ctypes.c_void_p], ctypes.c_int),
+    "ek_batch_count": ([ctypes.c_void_p, _P(ctypes.c_int32), _P(ctypes.c_int64)], ctypes.c_int),
+    "ek_batch_channel": ([ctypes.c_void_p, ctypes.c_int32, _P(ctypes.c_void_p)], ctypes.c_int),
+    "ek_batch_stream": ([ctypes.c_void_p, _P(ctypes.c_void_p)], ctypes.c_int),
+    "ek_batch_set_cycle": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32], ctypes.c_int),
+    "ek_batch_init_equilibrium": ([ctypes.c_void_p], ctypes.c_int),
+    "ek_batch_step": ([ctypes.c_void_p, ctypes.c_int32], ctypes.c_int),
+    "ek_batch_sync": ([ctypes.c_void_p], ctypes.c_int),
+    "ek_batch_step_count": ([ctypes.c_void_p, _P(ctypes.c_int64)], ctypes.c_int),
+    "ek_batch_launch_count": ([ctypes.c_void_p, _P(ctypes.c_int64)], ctypes.c_int),
+    "ek_batch_tile_width": ([ctypes.c_void_p, _P(ctypes.c_int32)], ctypes.c_int),
+    "ek_batch_set_tile_width": ([ctypes.c_void_p, ctypes.c_int32], ctypes.c_int),
+    "ek_batch_autotune": ([ctypes.c_void_p, ctypes.c_int32, _P(ctypes.c_int32), _dp], ctypes.c_int),
+    "ek_batch_residual": ([ctypes.c_void_p, ctypes.c_int32, _dp, _dp], ctypes.c_int),
 }
 
 

@@ -1,0 +1,118 @@
+"""Batches of independent channels stepped in lockstep (ek_batch_* of the C ABI).
+
+The reference runs one channel per process (main.cu); a Batch runs hundreds
+of channels of different sizes and parameters with four kernel launches per
+step for all of them.  Each channel is a Channel view (fields in and out,
+wall profiles, Poisson-Boltzmann start, residual) that is stepped only
+through the batch.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from ._lib import EkParams, check, lib
+from .channel import Channel
+
+
+class Batch:
+    def __init__(self, params_list):
+        self.params = [dict(p) for p in params_list]
+        if not self.params:
+            raise ValueError("a batch needs at least one channel")
+        arr = (EkParams * len(self.params))(*[EkParams.from_dict(p) for p in self.params])
+        h = ctypes.c_void_p()
+        check(lib().ek_batch_create(arr, len(self.params), ctypes.byref(h)))
+        self._h = h
+        self.channels = []
+        for i, p in enumerate(self.params):
+            ch = ctypes.c_void_p()
+            check(lib().ek_batch_channel(self._h, i, ctypes.byref(ch)))
+            self.channels.append(Channel._borrowed(ch, p, self))
+        n = ctypes.c_int64(0)
+        check(lib().ek_batch_count(self._h, None, ctypes.byref(n)))
+        self.nodes = int(n.value)
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            for ch in self.channels:
+                ch._h = None
+            check(lib().ek_batch_destroy(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __len__(self):
+        return len(self.channels)
+
+    def __getitem__(self, i):
+        return self.channels[i]
+
+    # -- stepping ---------------------------------------------------------
+    def set_cycle(self, steps=200, rebase=True, graph=True):
+        check(lib().ek_batch_set_cycle(self._h, int(steps), 1 if rebase else 0, 1 if graph else 0))
+
+    def init_equilibrium(self):
+        check(lib().ek_batch_init_equilibrium(self._h))
+
+    def step(self, n=1):
+        check(lib().ek_batch_step(self._h, int(n)))
+
+    def sync(self):
+        check(lib().ek_batch_sync(self._h))
+
+    @property
+    def steps(self):
+        v = ctypes.c_int64(0)
+        check(lib().ek_batch_step_count(self._h, ctypes.byref(v)))
+        return int(v.value)
+
+    @property
+    def launches(self):
+        v = ctypes.c_int64(0)
+        check(lib().ek_batch_launch_count(self._h, ctypes.byref(v)))
+        return int(v.value)
+
+    @property
+    def stream(self):
+        v = ctypes.c_void_p()
+        check(lib().ek_batch_stream(self._h, ctypes.byref(v)))
+        return int(v.value or 0)
+
+    @property
+    def tile_width(self):
+        v = ctypes.c_int32(0)
+        check(lib().ek_batch_tile_width(self._h, ctypes.byref(v)))
+        return int(v.value)
+
+    @tile_width.setter
+    def tile_width(self, w):
+        check(lib().ek_batch_set_tile_width(self._h, int(w)))
+
+    def autotune(self, steps=20):
+        """Time each tile width (advances the state); returns (chosen, {width: ms/step})."""
+        chosen = ctypes.c_int32(0)
+        ms = np.zeros(3)
+        check(lib().ek_batch_autotune(self._h, int(steps), ctypes.byref(chosen),
+                                      ms.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return int(chosen.value), dict(zip((64, 128, 256), ms.tolist()))
+
+    def residual(self, interval):
+        """Per-channel residuals (n, 5): u_x, c+, c-, psi, max (inf before the first snapshot)."""
+        out = np.zeros((len(self.channels), 5))
+        worst = np.zeros(5)
+        dp = ctypes.POINTER(ctypes.c_double)
+        check(lib().ek_batch_residual(self._h, int(interval), out.ctypes.data_as(dp), worst.ctypes.data_as(dp)))
+        return out

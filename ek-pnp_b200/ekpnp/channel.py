@@ -42,9 +42,24 @@ class Channel:
         h = ctypes.c_void_p()
         check(lib().ek_create(ctypes.byref(self._p), ctypes.byref(h)))
         self._h = h
+        self._owner = None
+
+    @classmethod
+    def _borrowed(cls, handle, params, owner):
+        """A view of a context owned by `owner` (a Batch): never destroyed here."""
+        ch = cls.__new__(cls)
+        ch.params = dict(params)
+        ch._p = EkParams.from_dict(ch.params)
+        ch.nx, ch.ny = int(ch._p.nx), int(ch._p.ny)
+        ch._h = handle
+        ch._owner = owner
+        return ch
 
     # -- lifetime ---------------------------------------------------------
     def close(self):
+        if getattr(self, "_owner", None) is not None:
+            self._h = None
+            return
         if getattr(self, "_h", None):
             check(lib().ek_destroy(self._h))
             self._h = None

@@ -64,3 +64,44 @@ def workload_params(name, storage=STORE_F64, extra_flags=0):
     w = WORKLOADS[name]
     return channel_params(w["nx"], w["ny"], kappa_h=w["kappa_h"], zeta=w["zeta"], ex=w["ex"],
                           diff=w["diff"], storage=storage, extra_flags=extra_flags)
+
+
+# Batched workload: channels of uneven size and physics.
+BATCH_NX = (64, 128, 256, 512, 1024)
+
+
+# Permittivity (lattice units) of the batched channels.  It sets the size of
+# the electric stress against the lattice pressure rho0*cs2: the osmotic
+# pressure of a double layer is 2 f_charge c0 (cosh(zeta) - 1) with
+# f_charge = eps kappa^2 / (2 c0).  With eps = 1 the thinnest layers of the
+# draw (kappa up to 1.6 per lattice spacing, |zeta| up to 4) push the fluid
+# density to 3x rho0 and 10 of the 512 channels diverge within 20 steps in the
+# reference's own update rules (FP64 CPU oracle, Poisson-Boltzmann start);
+# with eps = 0.01 every channel stays below 8% density change.  The
+# reference's SI set-up (LBM.h:49-74) sits lower still, near 1e-5.
+BATCH_EPS = 0.01
+
+
+def batch_specs(count=512, seed=2, nx_choices=BATCH_NX, ny_range=(32, 512), kappa_h_range=(1.0, 50.0),
+                zeta_range=(-4.0, -0.5), ex_range=(1e-5, 1e-3), diff_range=(0.02, 0.1), eps=BATCH_EPS):
+    """Channel descriptions of the batched workload, drawn with numpy
+    default_rng(seed), per channel in this order: nx from nx_choices, ny
+    uniform integer in ny_range (inclusive), kappa*H log-uniform, zeta
+    uniform, E_x log-uniform, D uniform."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(int(count)):
+        nx = int(rng.choice(np.asarray(nx_choices)))
+        ny = int(rng.integers(ny_range[0], ny_range[1] + 1))
+        kh = float(np.exp(rng.uniform(np.log(kappa_h_range[0]), np.log(kappa_h_range[1]))))
+        zeta = float(rng.uniform(*zeta_range))
+        ex = float(np.exp(rng.uniform(np.log(ex_range[0]), np.log(ex_range[1]))))
+        diff = float(rng.uniform(*diff_range))
+        out.append(dict(nx=nx, ny=ny, kappa_h=kh, zeta=zeta, ex=ex, diff=diff, eps=float(eps)))
+    return out
+
+
+def spec_params(spec, storage):
+    return channel_params(spec["nx"], spec["ny"], kappa_h=spec["kappa_h"], zeta=spec["zeta"], ex=spec["ex"],
+                          diff=spec["diff"], eps=spec.get("eps", 1.0), storage=storage)
+

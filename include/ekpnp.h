@@ -254,6 +254,49 @@ int ek_elapsed(ek_ctx *ctx, int32_t slot_a, int32_t slot_b, double *ms);
 /* Total number of kernels this context has launched. */
 int ek_launch_count(const ek_ctx *ctx, int64_t *out);
 
+/* ---- batches of independent channels ------------------------------------
+ * No counterpart in the reference (one channel per run of main.cu).  A batch
+ * steps many channels of different sizes and parameters in lockstep, four
+ * kernel launches per step for all of them: one persistent LBM kernel over a
+ * tile work-list and three batched Poisson passes.  Each channel is an ek_ctx
+ * owned by the batch (ek_batch_channel); use it for ek_set_fields,
+ * ek_set_wall_profile, ek_init_poisson_boltzmann, ek_get_fields and
+ * ek_residual, but step it only through the batch.  Per channel, a batch step
+ * gives the bits of ek_step with ek_set_rebase_interval(cycle) (cycle below).
+ * Channels: FP32 or FP16 storage (one for all), nx a power of two in
+ * [16, 4096], ny <= 8194, E derived from psi (no EK_FLAG_EXPLICIT_E).
+ * All calls on one batch use the batch's own stream (ek_batch_stream). */
+typedef struct ek_batch ek_batch;
+int ek_batch_create(const ek_params *params, int32_t count, ek_batch **out);
+int ek_batch_destroy(ek_batch *b);
+int ek_batch_count(const ek_batch *b, int32_t *count, int64_t *nodes);
+int ek_batch_channel(ek_batch *b, int32_t index, ek_ctx **out);
+int ek_batch_stream(const ek_batch *b, void **stream);
+/* Steps run in cycles of `steps` (even, >= 2; default 200): the last step of a
+ * cycle writes the moments and, if rebase != 0 (default), re-bases the
+ * shifted populations to the new row means.  use_graph != 0 (default) replays
+ * whole cycles from a CUDA graph captured on first use. */
+int ek_batch_set_cycle(ek_batch *b, int32_t steps, int32_t rebase, int32_t use_graph);
+/* ek_init_equilibrium of every channel from its fields; step count to 0. */
+int ek_batch_init_equilibrium(ek_batch *b);
+/* nsteps coupled steps of every channel; the moments (fields) are current
+ * when the call's work ends.  Asynchronous: ek_batch_sync waits. */
+int ek_batch_step(ek_batch *b, int32_t nsteps);
+int ek_batch_sync(ek_batch *b);
+int ek_batch_step_count(const ek_batch *b, int64_t *out);
+int ek_batch_launch_count(const ek_batch *b, int64_t *out);
+/* Threads per LBM block (64, 128 or 256): tile width min(width, nx), and
+ * width / min(width, nx) rows per tile. */
+int ek_batch_tile_width(const ek_batch *b, int32_t *width);
+int ek_batch_set_tile_width(ek_batch *b, int32_t width);
+/* Times `steps` steps at each tile width (the state advances by
+ * 3 (steps + 2) steps), keeps the fastest; ms3 (optional): ms per step of
+ * widths 64, 128, 256. */
+int ek_batch_autotune(ek_batch *b, int32_t steps, int32_t *chosen, double *ms3);
+/* ek_residual of every channel: out5 gets 5 doubles per channel (u_x, c+,
+ * c-, psi, max), worst5 (optional) the maxima over the channels. */
+int ek_batch_residual(ek_batch *b, int32_t interval, double *out5, double *worst5);
+
 #ifdef __cplusplus
 }
 #endif
