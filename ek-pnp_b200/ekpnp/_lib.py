@@ -55,6 +55,7 @@ _lib = None
 
 _P = ctypes.POINTER
 _dp = _P(ctypes.c_double)
+_fp = _P(ctypes.c_float)
 _SIGS = {
     "ek_version": ([], ctypes.c_int),
     "ek_status_string": ([ctypes.c_int], ctypes.c_char_p),
@@ -103,6 +104,18 @@ _SIGS = {
     "ek_batch_set_tile_width": ([ctypes.c_void_p, ctypes.c_int32], ctypes.c_int),
     "ek_batch_autotune": ([ctypes.c_void_p, ctypes.c_int32, _P(ctypes.c_int32), _dp], ctypes.c_int),
     "ek_batch_residual": ([ctypes.c_void_p, ctypes.c_int32, _dp, _dp], ctypes.c_int),
+    "ek_mlp_create": ([ctypes.c_int32, ctypes.c_uint64, _P(ctypes.c_void_p)], ctypes.c_int),
+    "ek_mlp_destroy": ([ctypes.c_void_p], ctypes.c_int),
+    "ek_mlp_param_count": ([ctypes.c_void_p, _P(ctypes.c_int64)], ctypes.c_int),
+    "ek_mlp_get_params": ([ctypes.c_void_p, _fp], ctypes.c_int),
+    "ek_mlp_set_params": ([ctypes.c_void_p, _fp], ctypes.c_int),
+    "ek_mlp_set_data": ([ctypes.c_void_p, _fp, _fp, ctypes.c_int64], ctypes.c_int),
+    "ek_mlp_train": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_float, _dp], ctypes.c_int),
+    "ek_mlp_gradients": ([ctypes.c_void_p, _fp, _fp, _fp, _dp], ctypes.c_int),
+    "ek_mlp_forward": ([ctypes.c_void_p, _fp, ctypes.c_int64, _fp], ctypes.c_int),
+    "ek_mlp_launch_count": ([ctypes.c_void_p, _P(ctypes.c_int64)], ctypes.c_int),
+    "ek_gemm_bf16": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+                      ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p], ctypes.c_int),
 }
 
 

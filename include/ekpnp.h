@@ -297,6 +297,42 @@ int ek_batch_autotune(ek_batch *b, int32_t steps, int32_t *chosen, double *ms3);
  * c-, psi, max), worst5 (optional) the maxima over the channels. */
 int ek_batch_residual(ek_batch *b, int32_t interval, double *out5, double *worst5);
 
+/* ---- learned warm start: MLP on the tensor cores ------------------------
+ * No counterpart in the reference.  A 4 -> 256 -> 256 -> 256 -> 512 network
+ * with SiLU activations (inputs: the four normalised channel descriptors;
+ * outputs: four 128-point profiles across the channel).  Forward, backward
+ * and Adam run in hand-written kernels: BF16 operands on the tensor cores
+ * (tcgen05, FP32 accumulation in tensor memory), FP32 master weights.
+ * Parameters are one flat FP32 array, per layer W (out x in, row-major; the
+ * first layer's 4 inputs padded to 16 with zero weights) then b (out). */
+typedef struct ek_mlp ek_mlp;
+/* batch: rows per training step, a multiple of 128; seed: weight
+ * initialisation (Glorot uniform, zero biases) and batch shuffling. */
+int ek_mlp_create(int32_t batch, uint64_t seed, ek_mlp **out);
+int ek_mlp_destroy(ek_mlp *m);
+int ek_mlp_param_count(const ek_mlp *m, int64_t *n);
+int ek_mlp_get_params(ek_mlp *m, float *flat);
+/* Replaces the parameters and resets the Adam state and step count. */
+int ek_mlp_set_params(ek_mlp *m, const float *flat);
+/* Training set: x n x 4, t n x 512 (host, FP32), n >= batch. */
+int ek_mlp_set_data(ek_mlp *m, const float *x, const float *t, int64_t n);
+/* iters Adam steps (beta1 0.9, beta2 0.999, eps 1e-8) on shuffled batches
+ * (a new permutation every epoch); loss_out (optional, iters doubles) gets
+ * each step's mean squared error. */
+int ek_mlp_train(ek_mlp *m, int32_t iters, float lr, double *loss_out);
+/* Gradients of the mean squared error of one batch (x batch x 4, t batch x
+ * 512) into grads (param_count floats), loss optional; no update. */
+int ek_mlp_gradients(ek_mlp *m, const float *x, const float *t, float *grads, double *loss);
+/* y (n x 512) = network(x (n x 4)), host arrays. */
+int ek_mlp_forward(ek_mlp *m, const float *x, int64_t n, float *y);
+int ek_mlp_launch_count(const ek_mlp *m, int64_t *out);
+/* C (m x n, FP32, row stride ldc) = A (m x k) * B (n x k)^T on the tensor
+ * cores; A, B BF16 (uint16 bit patterns), device pointers 16-byte aligned;
+ * m a multiple of 128, n a multiple of 16 (of 128 above 128), k a multiple of
+ * 16, lda and ldb multiples of 8.  Synchronises the stream. */
+int ek_gemm_bf16(const uint16_t *a, int32_t lda, const uint16_t *b, int32_t ldb, float *c, int32_t ldc,
+                 int32_t m, int32_t n, int32_t k, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
