@@ -28,6 +28,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <string>
 #include <vector>
 
@@ -604,9 +605,17 @@ int ek_batch_residual(ek_batch *b, int32_t interval, double *out5, double *worst
     EK_BCUDA(cudaStreamSynchronize(b->stream), "residual sync");
     double w[5] = {0, 0, 0, 0, 0};
     for (int i = 0; i < nch; ++i) {
-        const int rc = ek::ctx_residual_finish(b->ch[i], &h[(size_t)i * 8], interval, out5 + (size_t)i * 5);
+        double *o = out5 + (size_t)i * 5;
+        const double *sums = &h[(size_t)i * 8];
+        if (!std::all_of(sums, sums + 8, [](double v) { return std::isfinite(v); })) {
+            // a diverged channel: NaN residuals, the others carry on
+            std::fill(o, o + 5, std::nan(""));
+            b->ch[i]->snap_valid = false;
+            continue;
+        }
+        const int rc = ek::ctx_residual_finish(b->ch[i], sums, interval, o);
         if (rc != EK_OK) return rc;
-        for (int k = 0; k < 5; ++k) w[k] = std::max(w[k], out5[(size_t)i * 5 + k]);
+        for (int k = 0; k < 5; ++k) w[k] = std::max(w[k], o[k]);
     }
     if (worst5)
         for (int k = 0; k < 5; ++k) worst5[k] = w[k];

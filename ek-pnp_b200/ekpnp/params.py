@@ -75,11 +75,20 @@ BATCH_NX = (64, 128, 256, 512, 1024)
 # pressure of a double layer is 2 f_charge c0 (cosh(zeta) - 1) with
 # f_charge = eps kappa^2 / (2 c0).  With eps = 1 the thinnest layers of the
 # draw (kappa up to 1.6 per lattice spacing, |zeta| up to 4) push the fluid
-# density to 3x rho0 and 10 of the 512 channels diverge within 20 steps in the
-# reference's own update rules (FP64 CPU oracle, Poisson-Boltzmann start);
+# density to 2.9 rho0 and 10 of the 512 channels diverge within 300 steps in
+# the reference's own update rules (FP64 CPU oracle, Poisson-Boltzmann start);
 # with eps = 0.01 every channel stays below 8% density change.  The
 # reference's SI set-up (LBM.h:49-74) sits lower still, near 1e-5.
 BATCH_EPS = 0.01
+# The batched channels use the consistent rest equilibrium of the negative ion
+# (EK_FLAG_REST_QUIRK off: the drift velocity of c-, as the reference's own
+# initialisation does, LBM.cu:242).  With the quirk of gpu_collide_save
+# (LBM.cu:493) a slowly growing instability ends long runs: in the FP64 CPU
+# oracle a 16 x 115 channel of the draw (kappa*H 37.6, zeta -0.64, D 0.092)
+# blows up after 122,000 steps with it, and without it converges to a
+# residual of 1e-13.  The quirk stays the default of single channels, whose
+# parity tests pin the reference build.
+BATCH_REST_QUIRK = False
 
 
 def batch_specs(count=512, seed=2, nx_choices=BATCH_NX, ny_range=(32, 512), kappa_h_range=(1.0, 50.0),
@@ -97,11 +106,13 @@ def batch_specs(count=512, seed=2, nx_choices=BATCH_NX, ny_range=(32, 512), kapp
         zeta = float(rng.uniform(*zeta_range))
         ex = float(np.exp(rng.uniform(np.log(ex_range[0]), np.log(ex_range[1]))))
         diff = float(rng.uniform(*diff_range))
-        out.append(dict(nx=nx, ny=ny, kappa_h=kh, zeta=zeta, ex=ex, diff=diff, eps=float(eps)))
+        out.append(dict(nx=nx, ny=ny, kappa_h=kh, zeta=zeta, ex=ex, diff=diff, eps=float(eps),
+                        rest_quirk=BATCH_REST_QUIRK))
     return out
 
 
 def spec_params(spec, storage):
     return channel_params(spec["nx"], spec["ny"], kappa_h=spec["kappa_h"], zeta=spec["zeta"], ex=spec["ex"],
-                          diff=spec["diff"], eps=spec.get("eps", 1.0), storage=storage)
+                          diff=spec["diff"], eps=spec.get("eps", 1.0), rest_quirk=spec.get("rest_quirk", True),
+                          storage=storage)
 

@@ -1,0 +1,224 @@
+"""Learned warm start of batched channels (new; the reference starts every
+run from its Poisson-Boltzmann initialisation, LBM.cu:95-145, or a file).
+
+Pipeline:
+  1. steady states   the batched solver runs many channels (drawn from the
+                     batched workload's distributions) to a steady state,
+                     residual < tol; the cross-channel profiles of psi, c+, c-
+                     and u_x (row means; walls uniform along x) are encoded as
+                     four 128-point profiles on Chebyshev-Lobatto points of
+                     s = y / (ny - 1), which cluster at the walls where the
+                     double layers are.
+  2. training        the MLP (ekpnp.mlp: tcgen05 GEMMs, Adam) maps the four
+                     normalised descriptors (kappa*H, zeta, E_x, N_y) to those
+                     512 numbers.
+  3. warm start      a channel's fields are decoded from the network's output
+                     and the solver iterates from them to the same residual.
+                     The solver judges the start: a channel whose residual
+                     rises between two checks early on, or goes non-finite, is
+                     re-run from the uniform cold start.
+Profile encoding (all O(1)): psi / zeta, ln(c+/c0) / (-zeta), ln(c-/c0) / zeta,
+u_x / u_HS with u_HS = -eps zeta E_x / (rho0 nu) the Helmholtz-Smoluchowski
+speed (Boltzmann equilibrium and the electro-osmotic profile make the four
+nearly 1 - s-shaped curves of one double layer).
+"""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+
+from ._lib import STORE_F32
+from .batch import Batch
+from .params import spec_params
+
+NS = 128
+S = 0.5 * (1.0 - np.cos(np.pi * np.arange(NS) / (NS - 1)))  # Chebyshev-Lobatto points on [0, 1]
+RANGES = {"kappa_h": (1.0, 50.0), "zeta": (-4.0, -0.5), "ex": (1e-5, 1e-3), "ny": (32, 512)}
+
+
+def _lin(v, lo, hi):
+    return 2.0 * (v - lo) / (hi - lo) - 1.0
+
+
+def features(specs):
+    """(n, 4) float32: log kappa*H, zeta, log E_x, log N_y mapped to [-1, 1]."""
+    out = np.empty((len(specs), 4), dtype=np.float32)
+    for i, s in enumerate(specs):
+        out[i, 0] = _lin(np.log(s["kappa_h"]), *np.log(RANGES["kappa_h"]))
+        out[i, 1] = _lin(s["zeta"], *RANGES["zeta"])
+        out[i, 2] = _lin(np.log(s["ex"]), *np.log(RANGES["ex"]))
+        out[i, 3] = _lin(np.log(s["ny"]), *np.log(RANGES["ny"]))
+    return out
+
+
+def u_hs(p):
+    return -p["eps"] * p["zeta_lo"] * p["ext_x"] / (p["rho0"] * p["nu"])
+
+
+def encode(spec, prof):
+    """512 float32 targets from 1-D profiles (ny values each) of psi, cp, cn, ux."""
+    p = spec_params(spec, 0)
+    ny, z = spec["ny"], spec["zeta"]
+    y = S * (ny - 1)
+    grid = np.arange(ny)
+    cols = (prof["psi"] / z,
+            np.log(np.maximum(prof["cp"], 1e-300) / p["c0"]) / (-z),
+            np.log(np.maximum(prof["cn"], 1e-300) / p["c0"]) / z,
+            prof["ux"] / u_hs(p))
+    return np.concatenate([np.interp(y, grid, c) for c in cols]).astype(np.float32)
+
+
+def decode(spec, vec, nx=None):
+    """Fields (ny x nx) of a channel from 512 network outputs."""
+    p = spec_params(spec, 0)
+    nx = spec["nx"] if nx is None else nx
+    ny, z = spec["ny"], spec["zeta"]
+    t = np.asarray(vec, dtype=np.float64).reshape(4, NS)
+    s = np.arange(ny) / (ny - 1)
+    psi = z * np.interp(s, S, t[0])
+    psi[0] = psi[-1] = z
+    cp = p["c0"] * np.exp(-z * np.interp(s, S, t[1]))
+    cn = p["c0"] * np.exp(z * np.interp(s, S, t[2]))
+    ux = u_hs(p) * np.interp(s, S, t[3])
+    ux[0] = ux[-1] = 0.0
+    col = lambda v: np.repeat(v[:, None], nx, axis=1)
+    return dict(rho=np.full((ny, nx), p["rho0"]), ux=col(ux), uy=np.zeros((ny, nx)), cp=col(cp), cn=col(cn),
+                psi=col(psi))
+
+
+def profiles(ch):
+    """Row means of psi, cp, cn, ux of a channel."""
+    f = ch.get_fields(("psi", "cp", "cn", "ux"))
+    return {k: v.mean(axis=1) for k, v in f.items()}
+
+
+def cold_state(spec, nx=None):
+    p = spec_params(spec, 0)
+    nx = spec["nx"] if nx is None else nx
+    ny = spec["ny"]
+    z = np.zeros((ny, nx))
+    return dict(rho=np.full((ny, nx), p["rho0"]), ux=z, uy=z.copy(), cp=np.full((ny, nx), p["c0"]),
+                cn=np.full((ny, nx), p["c0"]), psi=z.copy())
+
+
+def physics_start(batch):
+    """Poisson-Boltzmann (Newton) ions and potential, the electro-osmotic
+    velocity u = u_HS (1 - psi/zeta) of that potential."""
+    for ch in batch:
+        ch.init_poisson_boltzmann("newton")
+        psi = ch.get_fields(("psi",))["psi"]
+        p = ch.params
+        ch.set_fields(ux=u_hs(p) * (1.0 - psi / p["zeta_lo"]))
+
+
+def run_to_steady(batch, tol=1e-8, check=1000, max_steps=200_000, judge=None):
+    """Step the batch until every channel has residual < tol (checked every
+    `check` steps) or diverged, or max_steps.  Returns per-channel steps to
+    steady (-1: not reached), a diverged mask, the residual history (one row
+    per check) and the wall time in seconds (host clock, checks included).
+    judge=(k1, k2): also return the channels whose worst residual rose from
+    check k1 to check k2."""
+    n = len(batch)
+    steps_to = np.full(n, -1, dtype=np.int64)
+    hist = []
+    batch.sync()
+    t0 = time.perf_counter()
+    batch.residual(check)  # first snapshot
+    while batch.steps < max_steps:
+        batch.step(min(check, max_steps - batch.steps))
+        r = batch.residual(check)[:, 4]
+        hist.append(r)
+        ok = np.isfinite(r)
+        newly = (steps_to < 0) & ok & (r < tol)
+        steps_to[newly] = batch.steps
+        if np.all((steps_to >= 0) | ~ok):
+            break
+    wall = time.perf_counter() - t0
+    hist = np.array(hist)
+    diverged = ~np.isfinite(hist[-1]) if len(hist) else np.zeros(n, bool)
+    rising = None if judge is None else rising_channels(hist, *judge)
+    return dict(steps=steps_to, diverged=diverged, history=hist, wall_s=wall, rising=rising)
+
+
+def rising_channels(hist, k1, k2):
+    """Channels whose residual at check k2 is above that at check k1, or that
+    are non-finite at any check so far (hist: checks x channels)."""
+    hist = np.asarray(hist, dtype=np.float64)
+    n = hist.shape[1]
+    bad = ~np.all(np.isfinite(hist), axis=0) if len(hist) else np.zeros(n, bool)
+    if len(hist) > k2:
+        with np.errstate(invalid="ignore"):
+            bad |= hist[k2] > hist[k1]
+    return bad
+
+
+def generate_steady_states(specs, nx=16, tol=1e-8, check=1000, max_steps=50_000, storage=STORE_F32, cycle=200):
+    """Targets (n x 512) of the channels described by specs, run from the
+    physics start on nx columns (walls uniform along x: the steady state does
+    not depend on x).  Returns (targets, converged mask, run info)."""
+    specs = [dict(s, nx=nx) for s in specs]
+    with Batch([spec_params(s, storage) for s in specs]) as b:
+        physics_start(b)
+        b.set_cycle(cycle)
+        b.init_equilibrium()
+        info = run_to_steady(b, tol=tol, check=check, max_steps=max_steps)
+        targets = np.stack([encode(s, profiles(ch)) for s, ch in zip(specs, b)])
+    conv = (info["steps"] >= 0) & np.all(np.isfinite(targets), axis=1)
+    return targets, conv, info
+
+
+def surrogate_fields(net, specs):
+    y = net.forward(features(specs))
+    return [decode(s, v) for s, v in zip(specs, y)]
+
+
+def warm_start_run(net, specs, tol=1e-8, check=1000, max_steps=200_000, storage=STORE_F32, cycle=200,
+                   judge=(1, 3)):
+    """Time to steady from the network's start, with the fallback to the cold
+    start for channels whose residual rises between checks judge[0] and
+    judge[1] (or that diverge).  Wall time covers inference, set-up of the
+    fields, both runs and their checks."""
+    t0 = time.perf_counter()
+    fields = surrogate_fields(net, specs)
+    with Batch([spec_params(s, storage) for s in specs]) as b:
+        for ch, f in zip(b, fields):
+            ch.set_fields(**f)
+        b.set_cycle(cycle)
+        b.init_equilibrium()
+        info = run_to_steady(b, tol=tol, check=check, max_steps=max_steps, judge=judge)
+        final = [profiles(ch) for ch in b]
+    fallback = np.nonzero(info["rising"])[0]
+    steps = info["steps"].copy()
+    steps[fallback] = -1
+    cold_info = None
+    if len(fallback):
+        sub = [specs[i] for i in fallback]
+        cold_info = cold_start_run(sub, tol=tol, check=check, max_steps=max_steps, storage=storage, cycle=cycle)
+        steps[fallback] = cold_info["steps"]
+    wall = time.perf_counter() - t0
+    return dict(steps=steps, wall_s=wall, first=info, fallback=fallback, cold=cold_info, fields=fields,
+                final=final)
+
+
+def cold_start_run(specs, tol=1e-8, check=1000, max_steps=200_000, storage=STORE_F32, cycle=200):
+    t0 = time.perf_counter()
+    with Batch([spec_params(s, storage) for s in specs]) as b:
+        for ch, s in zip(b, specs):
+            ch.set_fields(**cold_state(s))
+        b.set_cycle(cycle)
+        b.init_equilibrium()
+        info = run_to_steady(b, tol=tol, check=check, max_steps=max_steps)
+        info["final"] = [profiles(ch) for ch in b]
+    info["wall_s"] = time.perf_counter() - t0
+    return info
+
+
+def surrogate_error(spec, fields, prof):
+    """Max-abs error of the start against a converged profile, relative to the
+    converged field's max-abs, per field."""
+    out = {}
+    for k in ("psi", "cp", "cn", "ux"):
+        start = fields[k].mean(axis=1)
+        out[k] = float(np.abs(start - prof[k]).max() / max(np.abs(prof[k]).max(), 1e-300))
+    return out

@@ -294,7 +294,8 @@ int ek_batch_set_tile_width(ek_batch *b, int32_t width);
  * widths 64, 128, 256. */
 int ek_batch_autotune(ek_batch *b, int32_t steps, int32_t *chosen, double *ms3);
 /* ek_residual of every channel: out5 gets 5 doubles per channel (u_x, c+,
- * c-, psi, max), worst5 (optional) the maxima over the channels. */
+ * c-, psi, max), worst5 (optional) the maxima over the finite channels.  A
+ * channel holding non-finite values gets NaN residuals (the call succeeds). */
 int ek_batch_residual(ek_batch *b, int32_t interval, double *out5, double *worst5);
 
 /* ---- learned warm start: MLP on the tensor cores ------------------------

@@ -27,6 +27,7 @@ def test_spec_params_are_batchable():
         p = ekpnp.spec_params(s, ekpnp.STORE_F32)
         assert p["nx"] & (p["nx"] - 1) == 0 and 16 <= p["nx"] <= 4096
         assert p["storage"] == ekpnp.STORE_F32 and not p["flags"] & ekpnp.FLAG_EXPLICIT_E
+        assert not p["flags"] & ekpnp.FLAG_REST_QUIRK and p["flags"] & ekpnp.FLAG_FORCE
         assert p["eps"] == s["eps"] == ekpnp.params.BATCH_EPS
         assert abs(p["f_charge"] - p["eps"] * (s["kappa_h"] / (s["ny"] - 1)) ** 2 / 2) < 1e-15
         assert p["mob_p"] == s["diff"] and p["mob_n"] == -s["diff"]
