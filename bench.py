@@ -362,6 +362,89 @@ def run_batch(args, d):
     return 0
 
 
+def _start_summary(r, cap):
+    st = np.asarray(r["steps"])
+    ok = st >= 0
+    return {"wall_s": r["wall_s"], "converged": int(ok.sum()), "channels": int(len(st)),
+            "diverged": int(np.sum(r["diverged"])), "fallback": int(len(r["fallback"])),
+            "median_steps_converged": float(np.median(st[ok])) if ok.any() else None,
+            "steps_p90": float(np.percentile(np.where(ok, st, cap), 90)),
+            "mean_steps_capped": float(np.mean(np.where(ok, st, cap)))}
+
+
+def run_warmstart(args, d):
+    """Learned warm start: steady states of `train` channels (seed 3) from the
+    batched solver, the network trained on them (tensor-core kernels), then
+    time to residual < 1e-8 of `eval` held-out channels (seed 4) from the
+    network's start against the uniform cold start."""
+    import ekpnp
+    from ekpnp import batch_specs, warmstart as ws
+    if d.rank != 0:
+        return 0
+    ekpnp.set_device(d.local)
+    n_train = env_int("EK_WS_TRAIN", 8192)
+    n_eval = env_int("EK_WS_EVAL", 256)
+    cap = env_int("EK_WS_CAP", 200_000)
+    gen_cap = env_int("EK_WS_GEN_CAP", 120_000)
+    check = 2000
+    t0 = time.perf_counter()
+    tr = batch_specs(n_train, seed=3)
+    cache = os.environ.get("EK_WS_CACHE")
+    if cache and os.path.exists(cache):
+        z = np.load(cache)
+        T, conv, gen_steps = z["T"], z["conv"], z["steps"]
+    else:
+        T, conv, info = ws.generate_steady_states(tr, nx=16, max_steps=gen_cap, check=check)
+        gen_steps = info["steps"]
+        if cache:
+            np.savez(cache, T=T, conv=conv, steps=gen_steps)
+    gen_s = time.perf_counter() - t0
+    ok = np.all(np.isfinite(T), axis=1)
+    trs = [s for s, o in zip(tr, ok) if o]
+    ev = batch_specs(n_eval, seed=4)
+    kw = dict(max_steps=cap, check=check)
+    out, train = {}, {}
+    modes = os.environ.get("EK_WS_MODES", "residual,direct").split(",")
+    for mode in modes:
+        sg = ws.Surrogate(mode, seed=7)
+        t1 = time.perf_counter()
+        loss = sg.fit(trs, T[ok], iters=env_int("EK_WS_ITERS", 12000), lr=2e-3)
+        train[mode] = {"seconds": time.perf_counter() - t1, "final_loss": float(loss[-200:].mean()),
+                       "iterations": int(len(loss)), "gpu_launches": sg.net.launches}
+        r = ws.warm_start_run(sg, ev, **kw)
+        sg.close()
+        out[mode] = r
+    cold = ws.cold_start_run(ev, **kw)
+    best = modes[0]
+    # error of each start against the channel's final state of the warm run
+    errs = {}
+    for mode in modes:
+        e = np.array([[ws.surrogate_error(s, f, p)[q] for q in ("psi", "cp", "cn", "ux")]
+                      for s, f, p in zip(ev, out[mode]["fields"], out[best]["final"])])
+        errs[mode] = {q: {"median": float(np.median(e[:, i])), "max": float(e[:, i].max())}
+                      for i, q in enumerate(("psi", "cp", "cn", "ux"))}
+    both = (np.asarray(out[best]["steps"]) >= 0) & (np.asarray(cold["steps"]) >= 0)
+    line = {
+        "metric": "time_to_steady_s", "value": out[best]["wall_s"], "unit": "s", "higher_is_better": False,
+        "n_gpus": 1, "steps": None, "warmup": 0, "scaling": "none", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded channel draws; training from the batched solver's own steady states)",
+        "config": {"workload": f"warmstart-{n_eval}", "train_channels": n_train, "train_usable": int(ok.sum()),
+                   "train_converged": int(np.sum(conv)), "train_gen_cap": gen_cap, "eval_channels": n_eval,
+                   "tol": 1e-8, "cap_steps": cap, "check_every": check, "storage": "f32-shifted",
+                   "network": "4-256-256-256-512 SiLU, BF16 tcgen05, Adam"},
+        "generation_s": gen_s, "training": train,
+        "cold": _start_summary(cold, cap),
+        "surrogate": {m: _start_summary(out[m], cap) for m in modes},
+        "wall_speedup_vs_cold": {m: cold["wall_s"] / out[m]["wall_s"] for m in modes},
+        "median_step_ratio_both_converged": (float(np.median(np.asarray(cold["steps"])[both] /
+                                                             np.maximum(np.asarray(out[best]["steps"])[both], 1)))
+                                             if both.any() else None),
+        "start_error_vs_final": errs,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -370,6 +453,8 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", default="channel-4096x1024")
     ap.add_argument("--storage", choices=tuple(STORAGE), default="f32")
+    ap.add_argument("--warmstart", action="store_true",
+                    help="time to steady state from the learned warm start against the cold start")
     ap.add_argument("--batch", action="store_true",
                     help="the batched workload (512 uneven channels) instead of one channel")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -380,6 +465,8 @@ def main():
     try:
         if args.impl == "reference":
             rc = run_reference(args, d)
+        elif args.warmstart:
+            rc = run_warmstart(args, d)
         elif args.batch:
             args.workload = "batch-512"
             rc = run_batch(args, d)

@@ -102,14 +102,61 @@ def cold_state(spec, nx=None):
                 cn=np.full((ny, nx), p["c0"]), psi=z.copy())
 
 
-def physics_start(batch):
-    """Poisson-Boltzmann (Newton) ions and potential, the electro-osmotic
-    velocity u = u_HS (1 - psi/zeta) of that potential."""
-    for ch in batch:
-        ch.init_poisson_boltzmann("newton")
-        psi = ch.get_fields(("psi",))["psi"]
-        p = ch.params
-        ch.set_fields(ux=u_hs(p) * (1.0 - psi / p["zeta_lo"]))
+def pb_column(spec):
+    """Discrete 1-D Poisson-Boltzmann potential across the channel (the
+    equation of ek_init_poisson_boltzmann's Newton form):
+        (psi[j-1] - 2 psi[j] + psi[j+1]) / dy^2 + g (exp(-psi[j]) - exp(psi[j])) = 0,
+    psi = zeta on both walls, g = f_charge c0 / eps; damped Newton (each
+    update changes psi by at most 1) from the linear profile."""
+    from scipy.linalg import solve_banded
+    p = spec_params(spec, 0)
+    ny, z = spec["ny"], spec["zeta"]
+    g = p["f_charge"] * p["c0"] / p["eps"]
+    inv = 1.0 / (p["dy"] * p["dy"])
+    psi = np.full(ny, float(z))
+    ab = np.zeros((3, ny - 2))
+    polish = -1
+    for _ in range(500):
+        v = psi[1:-1]
+        em, ep = np.exp(-v), np.exp(v)
+        G = (psi[:-2] - 2.0 * v + psi[2:]) * inv + g * (em - ep)
+        ab[0, 1:] = inv
+        ab[1] = -2.0 * inv - g * (em + ep)
+        ab[2, :-1] = inv
+        d = solve_banded((1, 1), ab, -G)
+        m = float(np.abs(d).max())
+        damp = 1.0 / m if m > 1.0 else 1.0
+        psi[1:-1] += damp * d
+        if polish < 0 and damp == 1.0 and m < 1e-9 * max(abs(z), 1.0):
+            polish = 2
+        if polish >= 0:
+            polish -= 1
+            if polish < 0:
+                return psi
+    raise RuntimeError("Poisson-Boltzmann Newton iteration did not converge")
+
+
+def physics_profiles(spec):
+    """Poisson-Boltzmann ions and potential, and the electro-osmotic velocity
+    u = u_HS (1 - psi/zeta) of that potential (1-D profiles)."""
+    p = spec_params(spec, 0)
+    psi = pb_column(spec)
+    return dict(psi=psi, cp=p["c0"] * np.exp(-psi), cn=p["c0"] * np.exp(psi),
+                ux=u_hs(p) * (1.0 - psi / spec["zeta"]))
+
+
+def profile_fields(spec, prof, nx=None):
+    p = spec_params(spec, 0)
+    nx = spec["nx"] if nx is None else nx
+    ny = spec["ny"]
+    col = lambda v: np.repeat(np.asarray(v, dtype=np.float64)[:, None], nx, axis=1)
+    return dict(rho=np.full((ny, nx), p["rho0"]), ux=col(prof["ux"]), uy=np.zeros((ny, nx)), cp=col(prof["cp"]),
+                cn=col(prof["cn"]), psi=col(prof["psi"]))
+
+
+def physics_start(batch, specs):
+    for ch, s in zip(batch, specs):
+        ch.set_fields(**profile_fields(s, physics_profiles(s), nx=ch.nx))
 
 
 def run_to_steady(batch, tol=1e-8, check=1000, max_steps=200_000, judge=None):
@@ -159,7 +206,7 @@ def generate_steady_states(specs, nx=16, tol=1e-8, check=1000, max_steps=50_000,
     not depend on x).  Returns (targets, converged mask, run info)."""
     specs = [dict(s, nx=nx) for s in specs]
     with Batch([spec_params(s, storage) for s in specs]) as b:
-        physics_start(b)
+        physics_start(b, specs)
         b.set_cycle(cycle)
         b.init_equilibrium()
         info = run_to_steady(b, tol=tol, check=check, max_steps=max_steps)
@@ -168,19 +215,60 @@ def generate_steady_states(specs, nx=16, tol=1e-8, check=1000, max_steps=50_000,
     return targets, conv, info
 
 
-def surrogate_fields(net, specs):
-    y = net.forward(features(specs))
-    return [decode(s, v) for s, v in zip(specs, y)]
+class Surrogate:
+    """The warm-start network and its target encoding.
+
+    mode "direct": the network's 512 outputs are the encoded profiles.
+    mode "residual": they are the difference between the encoded steady
+    profiles and the encoded physics start (Poisson-Boltzmann ions and
+    potential, electro-osmotic velocity), scaled per output by its spread over
+    the training set; the start is the physics profiles plus that learned
+    correction of what the lattice's own steady state does differently."""
+
+    def __init__(self, mode="direct", batch=256, seed=0):
+        from .mlp import Mlp
+        if mode not in ("direct", "residual"):
+            raise ValueError("mode is 'direct' or 'residual'")
+        self.mode = mode
+        self.net = Mlp(batch=batch, seed=seed)
+        self.offset = np.zeros(4 * NS, dtype=np.float32)
+        self.scale = np.ones(4 * NS, dtype=np.float32)
+
+    def close(self):
+        self.net.close()
+
+    def _base(self, specs):
+        if self.mode == "direct":
+            return np.zeros((len(specs), 4 * NS), dtype=np.float32)
+        return np.stack([encode(s, physics_profiles(s)) for s in specs])
+
+    def fit(self, specs, targets, iters=8000, lr=2e-3, chunks=8):
+        """Adam with a cosine learning-rate decay in `chunks` steps; returns the
+        per-iteration losses (of the scaled targets)."""
+        y = targets - self._base(specs)
+        self.offset = y.mean(axis=0).astype(np.float32)
+        self.scale = np.maximum(y.std(axis=0), 1e-6).astype(np.float32)
+        self.net.set_data(features(specs), (y - self.offset) / self.scale)
+        losses = []
+        per = max(1, iters // chunks)
+        for k in range(chunks):
+            rate = lr * max(0.5 * (1.0 + np.cos(np.pi * k / chunks)), 0.02)
+            losses.append(self.net.train(per, rate))
+        return np.concatenate(losses)
+
+    def predict(self, specs):
+        return self._base(specs) + self.net.forward(features(specs)) * self.scale + self.offset
+
+    def fields(self, specs):
+        return [decode(s, v) for s, v in zip(specs, self.predict(specs))]
 
 
-def warm_start_run(net, specs, tol=1e-8, check=1000, max_steps=200_000, storage=STORE_F32, cycle=200,
-                   judge=(1, 3)):
-    """Time to steady from the network's start, with the fallback to the cold
-    start for channels whose residual rises between checks judge[0] and
-    judge[1] (or that diverge).  Wall time covers inference, set-up of the
-    fields, both runs and their checks."""
+def start_run(specs, fields, tol=1e-8, check=1000, max_steps=200_000, storage=STORE_F32, cycle=200, judge=None):
+    """Run the channels from the given start fields to steady state.  With
+    judge=(k1, k2) the channels whose residual rises between checks k1 and k2,
+    or that diverge, are re-run from the uniform cold start (their steps then
+    count from that start; the wall time covers both runs)."""
     t0 = time.perf_counter()
-    fields = surrogate_fields(net, specs)
     with Batch([spec_params(s, storage) for s in specs]) as b:
         for ch, f in zip(b, fields):
             ch.set_fields(**f)
@@ -188,30 +276,42 @@ def warm_start_run(net, specs, tol=1e-8, check=1000, max_steps=200_000, storage=
         b.init_equilibrium()
         info = run_to_steady(b, tol=tol, check=check, max_steps=max_steps, judge=judge)
         final = [profiles(ch) for ch in b]
-    fallback = np.nonzero(info["rising"])[0]
     steps = info["steps"].copy()
-    steps[fallback] = -1
-    cold_info = None
+    fallback = np.nonzero(info["rising"])[0] if judge is not None else np.zeros(0, dtype=np.int64)
+    cold = None
     if len(fallback):
         sub = [specs[i] for i in fallback]
-        cold_info = cold_start_run(sub, tol=tol, check=check, max_steps=max_steps, storage=storage, cycle=cycle)
-        steps[fallback] = cold_info["steps"]
-    wall = time.perf_counter() - t0
-    return dict(steps=steps, wall_s=wall, first=info, fallback=fallback, cold=cold_info, fields=fields,
-                final=final)
+        cold = start_run(sub, [cold_state(s) for s in sub], tol=tol, check=check, max_steps=max_steps,
+                         storage=storage, cycle=cycle)
+        steps[fallback] = cold["steps"]
+        for j, i in enumerate(fallback):
+            final[i] = cold["final"][j]
+    return dict(steps=steps, wall_s=time.perf_counter() - t0, first=info, fallback=fallback, cold=cold,
+                final=final, diverged=info["diverged"])
 
 
-def cold_start_run(specs, tol=1e-8, check=1000, max_steps=200_000, storage=STORE_F32, cycle=200):
+def warm_start_run(surrogate, specs, judge=(1, 3), **kw):
+    """Time to steady from the network's start with the cold-start fallback;
+    the wall time includes inference and decoding."""
     t0 = time.perf_counter()
-    with Batch([spec_params(s, storage) for s in specs]) as b:
-        for ch, s in zip(b, specs):
-            ch.set_fields(**cold_state(s))
-        b.set_cycle(cycle)
-        b.init_equilibrium()
-        info = run_to_steady(b, tol=tol, check=check, max_steps=max_steps)
-        info["final"] = [profiles(ch) for ch in b]
-    info["wall_s"] = time.perf_counter() - t0
-    return info
+    fields = surrogate.fields(specs)
+    out = start_run(specs, fields, judge=judge, **kw)
+    out["wall_s"] = time.perf_counter() - t0
+    out["fields"] = fields
+    return out
+
+
+def cold_start_run(specs, **kw):
+    return start_run(specs, [cold_state(s) for s in specs], **kw)
+
+
+def physics_start_run(specs, **kw):
+    t0 = time.perf_counter()
+    fields = [profile_fields(s, physics_profiles(s)) for s in specs]
+    out = start_run(specs, fields, **kw)
+    out["wall_s"] = time.perf_counter() - t0
+    out["fields"] = fields
+    return out
 
 
 def surrogate_error(spec, fields, prof):

@@ -50,3 +50,17 @@ def test_fallback_rule():
     bad = ws.rising_channels(hist, 1, 3)
     assert bad.tolist() == [False, True, True, True]
     assert ws.rising_channels(hist[:2], 1, 3).tolist() == [False, False, False, True]
+
+
+def test_pb_column_solves_the_discrete_equation():
+    import ekpnp
+    from ekpnp import spec_params, warmstart as ws
+    for s in ekpnp.batch_specs(16, seed=7):
+        psi = ws.pb_column(s)
+        p = spec_params(s, 0)
+        g = p["f_charge"] * p["c0"] / p["eps"]
+        lap = psi[:-2] - 2 * psi[1:-1] + psi[2:]
+        src = g * (np.exp(-psi[1:-1]) - np.exp(psi[1:-1]))
+        # rounding of the second difference of O(|zeta|) values bounds the residual
+        assert np.abs(lap + src).max() <= 1e-14 * max(abs(s["zeta"]), 1.0) * 8
+        assert psi[0] == psi[-1] == s["zeta"] and np.all(np.diff(psi[: len(psi) // 2]) >= 0)
