@@ -445,6 +445,134 @@ def run_warmstart(args, d):
     return 0
 
 
+def run_hetero(args, d):
+    """Heterogeneous wall: one 8192 x 2048 channel, zeta(x) = -2 + 1.5 sin(2 pi x / 1024),
+    kappa*H = 64, E_x = 1e-4, seed 5.  FP32 shifted from a warm start (the
+    residual surrogate at the mean zeta when a training cache is given in
+    EK_WS_CACHE, else the per-column Poisson-Boltzmann/electro-osmotic physics
+    start) against the FP64 path from the uniform cold start: MLUPS, LBM
+    roofline, FP32 error against FP64 from the same start, residual after a
+    step cap."""
+    import ekpnp
+    from ekpnp import Channel, channel_params, noisy_uniform_state, warmstart as ws
+    if d.rank != 0:
+        return 0
+    ekpnp.set_device(d.local)
+    nx, ny = env_int("EK_HET_NX", 8192), env_int("EK_HET_NY", 2048)
+    K = args.steps
+    cap = env_int("EK_HET_CAP", 20000)
+    check = 1000
+    spec = dict(nx=nx, ny=ny, kappa_h=64.0, zeta=-2.0, ex=1e-4, diff=0.05, eps=0.01, rest_quirk=False)
+    x = np.arange(nx)
+    zeta = -2.0 + 1.5 * np.sin(2 * np.pi * x / 1024.0)
+    walls = dict(zeta_lo=zeta, zeta_hi=zeta, cp_lo=np.exp(-zeta), cp_hi=np.exp(-zeta), cn_lo=np.exp(zeta),
+                 cn_hi=np.exp(zeta))
+
+    def make(storage):
+        p = ekpnp.spec_params(spec, storage)
+        ch = Channel(p)
+        ch.set_wall_profile(**walls)
+        if storage != ekpnp.STORE_F64:
+            ch.set_rebase_interval(200)
+        return ch
+
+    # warm start fields
+    cache = os.environ.get("EK_WS_CACHE")
+    if cache and os.path.exists(cache):
+        from ekpnp import batch_specs
+        z = np.load(cache)
+        tr = batch_specs(len(z["T"]), seed=3)
+        ok = np.all(np.isfinite(z["T"]), axis=1)
+        sg = ws.Surrogate("residual", seed=7)
+        sg.fit([s_ for s_, o in zip(tr, ok) if o], z["T"][ok], iters=12000, lr=2e-3)
+        warm = sg.fields([spec])[0]
+        sg.close()
+        start_kind = "residual surrogate at the mean zeta"
+    else:
+        with make(ekpnp.STORE_F32) as ch:
+            ch.init_poisson_boltzmann("newton")
+            warm = ch.get_fields(("rho", "ux", "uy", "cp", "cn", "psi"))
+        u = ws.u_hs(ekpnp.spec_params(spec, 0)) / spec["zeta"] * (zeta[None, :] - warm["psi"])
+        warm["ux"] = u
+        start_kind = "per-column Poisson-Boltzmann + electro-osmotic velocity"
+
+    def timed_run(ch, steps):
+        ch.sync()
+        ch.mark(0)
+        ch.step(steps)
+        ch.mark(1)
+        ms = ch.elapsed_ms(0, 1)
+        return ms
+
+    out = {}
+    # FP32 from the warm start: MLUPS, roofline, then to the cap
+    with make(ekpnp.STORE_F32) as ch:
+        ch.set_fields(**warm)
+        ch.init_equilibrium()
+        ch.step(args.warmup)
+        ms = timed_run(ch, K)
+        ch.profile(True)
+        ch.step(min(K, 200))
+        prof = ch.profile_read()
+        ch.profile(False)
+        f32_k = ch.get_fields(("ux", "cp", "cn", "psi"))
+        lbm_ms, lbm_n = prof["lbm"]
+        per = lbm_ms / max(lbm_n, 1) / 1e3
+        peak, kind = measured_peak_gbs()
+        out["f32_warm"] = {"mlups": nx * ny * K / (ms / 1e3) / 1e6, "ms_per_step": ms / K,
+                           "lbm_launch_ms": per * 1e3, "lbm_gbs": nx * ny * 232 / per / 1e9,
+                           "lbm_frac": nx * ny * 232 / per / 1e9 / peak, "peak_kind": kind}
+        t0 = time.perf_counter()
+        ch.residual(check)
+        hist = []
+        while ch.steps < cap:
+            ch.step(check)
+            hist.append(float(ch.residual(check)[4]))
+            if hist[-1] < 1e-8:
+                break
+        out["f32_warm"].update({"steps": int(ch.steps), "residual": hist[-1] if hist else None,
+                                "wall_s": time.perf_counter() - t0})
+    # FP64 from the same warm start: error of FP32 after K + warmup + 200 steps
+    with make(ekpnp.STORE_F64) as ch:
+        ch.set_fields(**warm)
+        ch.init_equilibrium()
+        ch.step(args.warmup + K + min(K, 200))
+        f64_k = ch.get_fields(("ux", "cp", "cn", "psi"))
+    out["f32_error_vs_f64"] = {k: float(np.abs(f32_k[k] - f64_k[k]).max() / np.abs(f64_k[k]).max())
+                               for k in f64_k}
+    # FP64 from the uniform cold start
+    with make(ekpnp.STORE_F64) as ch:
+        ch.set_fields(**noisy_uniform_state(nx, ny, seed=5))
+        ch.init_equilibrium()
+        ch.step(args.warmup)
+        ms = timed_run(ch, K)
+        out["f64_cold"] = {"mlups": nx * ny * K / (ms / 1e3) / 1e6, "ms_per_step": ms / K}
+        t0 = time.perf_counter()
+        ch.residual(check)
+        hist = []
+        while ch.steps < cap:
+            ch.step(check)
+            try:
+                r = ch.residual(check)[4]
+            except ekpnp.EkError:  # non-finite fields: the cold start diverged
+                r = float("nan")
+            hist.append(float(r))
+            if not np.isfinite(r) or r < 1e-8:
+                break
+        out["f64_cold"].update({"steps": int(ch.steps), "residual": hist[-1] if hist else None,
+                                "wall_s": time.perf_counter() - t0})
+    line = {"metric": "coupled_mlups", "value": out["f32_warm"]["mlups"], "unit": "MLUPS", "n_gpus": 1,
+            "steps": K, "warmup": args.warmup, "ms_per_step": out["f32_warm"]["ms_per_step"],
+            "higher_is_better": True, "scaling": "none", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seed 5 noise for the cold start)",
+            "config": {"workload": f"hetero-wall-{nx}x{ny}", "kappa_h": 64.0, "e_x": 1e-4,
+                       "zeta": "-2 + 1.5 sin(2 pi x / 1024)", "eps": 0.01, "rest_quirk": False,
+                       "warm_start": start_kind, "cap_steps": cap, "tol": 1e-8},
+            **out}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -453,6 +581,8 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", default="channel-4096x1024")
     ap.add_argument("--storage", choices=tuple(STORAGE), default="f32")
+    ap.add_argument("--hetero", action="store_true",
+                    help="the 8192 x 2048 heterogeneous-wall channel: FP32 warm start against FP64 cold start")
     ap.add_argument("--warmstart", action="store_true",
                     help="time to steady state from the learned warm start against the cold start")
     ap.add_argument("--batch", action="store_true",
@@ -465,6 +595,8 @@ def main():
     try:
         if args.impl == "reference":
             rc = run_reference(args, d)
+        elif args.hetero:
+            rc = run_hetero(args, d)
         elif args.warmstart:
             rc = run_warmstart(args, d)
         elif args.batch:
