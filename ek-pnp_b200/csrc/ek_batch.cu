@@ -44,8 +44,13 @@ constexpr int REFS_TPB = 256;
 // ---- kernels ---------------------------------------------------------------
 
 // Persistent LBM kernel over the tile list; TXB threads = tile width x rows.
+// Threads per SM the register allocation must allow (896: the single-channel
+// kernel's 7 blocks of 128 threads, 72 registers).
+#ifndef EK_BATCH_SM_THREADS
+#define EK_BATCH_SM_THREADS 896
+#endif
 template <typename S, bool FIRST, bool EE, int TXB>
-__global__ void __launch_bounds__(TXB)
+__global__ void __launch_bounds__(TXB, (EK_BATCH_SM_THREADS / TXB) > 0 ? (EK_BATCH_SM_THREADS / TXB) : 1)
 batch_lbm(const ChanF *__restrict__ chans, const S *const *__restrict__ src, S *const *__restrict__ dst,
           double *const *__restrict__ fields, const int4 *__restrict__ tiles, int ntiles, bool mom) {
     __shared__ ChanF ks;
@@ -160,6 +165,8 @@ bool pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
 struct ek_batch {
     std::vector<ek_ctx *> ch;
     std::vector<int> kcur;           // each channel's current reference buffer when the tables were built
+    std::vector<char> active;        // channels that step (frozen ones keep their state)
+    std::vector<int64_t> ch_steps;   // steps each channel has taken in the batch
     int storage = EK_STORE_F32;
     cudaStream_t stream = nullptr;
     int cur = 0;                     // population buffer holding the current state (all channels)
@@ -232,6 +239,7 @@ void release_graph(ek_batch *b) {
 int build_tiles(ek_batch *b, int txb) {
     std::vector<int4> tiles;
     for (size_t i = 0; i < b->ch.size(); ++i) {
+        if (!b->active[i]) continue;
         const ek_params &p = b->ch[i]->p;
         const int w = std::min(txb, p.nx);
         const int rows = txb / w;
@@ -281,11 +289,13 @@ int build_tables(ek_batch *b) {
         sp.push_back(c->kref[c->kcur ^ 1]);
         kq.push_back(make_int4(c->kq[0], c->kq[1], c->kq[2], 0));
         const int nx = c->p.nx, n = c->pp.n;
-        const int per = 256 / (nx >> 4);
-        for (int q = 0; q < (n + 1) / 2; q += per) pairs.push_back(make_int2((int)i, q));
-        const int M = poisson_tridiag_modes(n);
-        for (int m0 = 0; m0 <= nx / 2; m0 += M) modes.push_back(make_int3((int)i, m0, M));
-        for (int y = 0; y < c->p.ny; ++y) rows.push_back(make_int2((int)i, y));
+        if (b->active[i]) {
+            const int per = 256 / (nx >> 4);
+            for (int q = 0; q < (n + 1) / 2; q += per) pairs.push_back(make_int2((int)i, q));
+            const int M = poisson_tridiag_modes(n);
+            for (int m0 = 0; m0 <= nx / 2; m0 += M) modes.push_back(make_int3((int)i, m0, M));
+            for (int y = 0; y < c->p.ny; ++y) rows.push_back(make_int2((int)i, y));
+        }
         const int nb = residual_blocks(c->chan);
         for (int k = 0; k < nb; ++k) ritems.push_back(make_int4((int)i, k, nb, nrpart));
         rranges.push_back(make_int2(nrpart, nb));
@@ -337,6 +347,7 @@ int launch_step(ek_batch *b, bool first, bool ee, bool mom) {
 
 // Re-base every channel's current populations to its new row means, in place.
 int launch_rebase(ek_batch *b) {
+    if (b->nrows == 0) return EK_OK;  // every channel frozen
     batch_row_refs<<<b->nrows, REFS_TPB, 0, b->stream>>>(b->d_chanf, b->d_fields, b->d_kq, b->d_spare, b->d_rows);
     EK_BCUDA(cudaGetLastError(), "batch row references");
     void *pops = b->d_pops[b->cur];
@@ -378,12 +389,16 @@ int capture_graph(ek_batch *b) {
     return EK_OK;
 }
 
-void sync_channel_state(ek_batch *b) {
-    for (ek_ctx *c : b->ch) {
+// Per-channel state after `advanced` batch steps of the active channels.
+void sync_channel_state(ek_batch *b, int64_t advanced) {
+    for (size_t i = 0; i < b->ch.size(); ++i) {
+        if (!b->active[i]) continue;
+        ek_ctx *c = b->ch[i];
+        b->ch_steps[i] += advanced;
         c->cur = b->cur;
         c->state_pre = b->state_pre;
         c->explicit_e_once = b->explicit_e_once;
-        c->steps = b->steps;
+        c->steps = b->ch_steps[i];
         c->e_stale = true;
     }
 }
@@ -394,7 +409,8 @@ int check_channels(ek_batch *b) {
     for (size_t i = 0; i < b->ch.size(); ++i) {
         const ek_ctx *c = b->ch[i];
         if (!c->initialised) return ek::ctx_fail(EK_ERR_INVALID, "call ek_batch_init_equilibrium before stepping");
-        if (c->cur != b->cur || c->kcur != b->kcur[i] || c->steps != b->steps)
+        if (!b->active[i]) continue;
+        if (c->cur != b->cur || c->kcur != b->kcur[i] || c->steps != b->ch_steps[i])
             return ek::ctx_fail(EK_ERR_INVALID,
                                 "a channel was stepped or re-based on its own; call ek_batch_init_equilibrium");
     }
@@ -440,6 +456,8 @@ int ek_batch_create(const ek_params *params, int32_t count, ek_batch **out) {
             return rc;
         }
         b->ch.push_back(c);
+        b->active.push_back(1);
+        b->ch_steps.push_back(0);
         b->nodes += (int64_t)params[i].nx * params[i].ny;
     }
     int rc = build_tables(b);
@@ -496,6 +514,8 @@ int ek_batch_init_equilibrium(ek_batch *b) {
     // one first-step variant for all: if any channel carries explicit E
     // (reference Poisson-Boltzmann start, fields loaded with E), the others get
     // the E of their psi written to their E planes
+    std::fill(b->active.begin(), b->active.end(), 1);
+    std::fill(b->ch_steps.begin(), b->ch_steps.end(), 0);
     bool ee = false;
     for (ek_ctx *c : b->ch) ee = ee || c->explicit_e_once;
     for (ek_ctx *c : b->ch) {
@@ -511,9 +531,10 @@ int ek_batch_init_equilibrium(ek_batch *b) {
     b->explicit_e_once = ee;
     b->steps = 0;
     int rc = build_tables(b);  // reference buffers may have changed
+    if (rc == EK_OK) rc = build_tiles(b, b->txb);
     if (rc != EK_OK) return rc;
     EK_BCUDA(cudaStreamSynchronize(b->stream), "batch init");
-    sync_channel_state(b);
+    sync_channel_state(b, 0);
     return EK_OK;
 }
 
@@ -548,7 +569,7 @@ int ek_batch_step(ek_batch *b, int32_t nsteps) {
         ++done;
         ++b->steps;
     }
-    sync_channel_state(b);
+    sync_channel_state(b, done);
     return EK_OK;
 }
 
@@ -586,6 +607,40 @@ int ek_batch_set_tile_width(ek_batch *b, int32_t width) {
 int ek_batch_stream(const ek_batch *b, void **out) {
     if (!b || !out) return ek::ctx_fail(EK_ERR_INVALID, "null argument");
     *out = (void *)b->stream;
+    return EK_OK;
+}
+
+// Channels with mask[i] == 0 stop stepping and keep their state (and step
+// count); mask[i] != 0 steps them again, which needs their state in the
+// batch's current buffer parity (an even number of batch steps since they
+// were frozen).  Launches per step stay four; the work shrinks to the active
+// channels.
+int ek_batch_set_active(ek_batch *b, const uint8_t *mask) {
+    if (!b || !mask) return ek::ctx_fail(EK_ERR_INVALID, "null argument");
+    EK_BCUDA(cudaStreamSynchronize(b->stream), "batch sync");
+    for (size_t i = 0; i < b->ch.size(); ++i)
+        if (mask[i] && !b->active[i] && b->ch[i]->cur != b->cur)
+            return ek::ctx_fail(EK_ERR_INVALID, "a frozen channel can rejoin only after an even number of batch steps");
+    bool changed = false;
+    for (size_t i = 0; i < b->ch.size(); ++i) {
+        const char a = mask[i] ? 1 : 0;
+        changed = changed || a != b->active[i];
+        b->active[i] = a;
+    }
+    if (!changed) return EK_OK;
+    int rc = build_tables(b);
+    if (rc == EK_OK) rc = build_tiles(b, b->txb);
+    return rc;
+}
+
+int ek_batch_active(const ek_batch *b, uint8_t *mask, int64_t *active_nodes) {
+    if (!b) return ek::ctx_fail(EK_ERR_INVALID, "null batch");
+    int64_t n = 0;
+    for (size_t i = 0; i < b->ch.size(); ++i) {
+        if (mask) mask[i] = (uint8_t)b->active[i];
+        if (b->active[i]) n += (int64_t)b->ch[i]->p.nx * b->ch[i]->p.ny;
+    }
+    if (active_nodes) *active_nodes = n;
     return EK_OK;
 }
 

@@ -42,6 +42,9 @@ struct ChanF {
     // FP64 constants of the fluid relaxation + Guo source (see node_shifted)
     double wpd, wmd, spd, smd, kcud, hinvcs2d, gFd, inv_cs2d, dtd;
     double f_charge, eps, ext_x, exf, dx, dy;
+    double half_inv_dx, half_inv_dy;   // E = (psi[-] - psi[+]) * (1/(2 dx)), one multiply each
+    double rhs_q;                      // -f_charge / eps: Poisson right-hand side per unit c+ - c-
+    double inv_dy2;                    // 1/dy^2 of the wall lifting term
     const double *zlo, *zhi, *cplo, *cphi, *cnlo, *cnhi;
     const float *kref;               // per-row references / 36 (see Chan::kref)
 };
@@ -185,12 +188,16 @@ __device__ __forceinline__ void add_guo(T d[9], T ux, T uy, T fx, T fy, const Co
     pair(d[6], d[8], wd, cuy - cux, cfy - cfx, gy - gx);
 }
 
-__device__ __forceinline__ void efield_at_d(const double *__restrict__ psi, int nxp, int ny, double dx, double dy,
-                                            int x, int y, int xm, int xp, double *ex, double *ey) {
-    const size_t r = (size_t)y * nxp;
-    *ex = 0.5 * (__ldg(psi + r + xm) - __ldg(psi + r + xp)) / dx;
-    const int yc = y == 0 ? 1 : (y == ny - 1 ? ny - 2 : y);
-    *ey = 0.5 * (__ldg(psi + (size_t)(yc - 1) * nxp + x) - __ldg(psi + (size_t)(yc + 1) * nxp + x)) / dy;
+// Central-difference E of the shifted forms (the stencil of gpu_efield and
+// gpu_bc, poisson.cu:145-174: wall rows take the adjacent row's Ey), with
+// the 1/(2 dx), 1/(2 dy) factors precomputed: a multiply in place of an
+// FP64 division per component.
+__device__ __forceinline__ void efield_shifted(const ChanF &k, const double *__restrict__ psi, int x, int y, int xm,
+                                               int xp, double *ex, double *ey) {
+    const size_t r = (size_t)y * k.nxp;
+    *ex = (__ldg(psi + r + xm) - __ldg(psi + r + xp)) * k.half_inv_dx;
+    const int yc = y == 0 ? 1 : (y == k.ny - 1 ? k.ny - 2 : y);
+    *ey = (__ldg(psi + (size_t)(yc - 1) * k.nxp + x) - __ldg(psi + (size_t)(yc + 1) * k.nxp + x)) * k.half_inv_dy;
 }
 
 // One node of one step.  src/dst: 27 population planes (species-major);
@@ -269,7 +276,7 @@ __device__ __forceinline__ void collide_shifted(const ChanF &k, float f[9], floa
         exd = fields[F_EX * pl + o];
         eyd = fields[F_EY * pl + o];
     } else {
-        efield_at_d(fields + F_PSI * pl, nxp, k.ny, k.dx, k.dy, x, y, xm, xp, &exd, &eyd);
+        efield_shifted(k, fields + F_PSI * pl, x, y, xm, xp, &exd, &eyd);
     }
     const float Ex = (float)exd, Ey = (float)eyd;
     float fx = 0.0f, fy = 0.0f;
@@ -279,8 +286,9 @@ __device__ __forceinline__ void collide_shifted(const ChanF &k, float f[9], floa
         fx = (float)(q * (exd + k.ext_x) + k.exf);
         fy = (float)(q * eyd);
     }
-    float ux = (momx(f) * k.inv_cfl + fx * k.half_dt) / rho;
-    float uy = (momy(f) * k.inv_cfl + fy * k.half_dt) / rho;
+    const float rrho = 1.0f / rho;
+    float ux = (momx(f) * k.inv_cfl + fx * k.half_dt) * rrho;
+    float uy = (momy(f) * k.inv_cfl + fy * k.half_dt) * rrho;
     if (lo) {
         float m[9];
         const size_t o1 = (size_t)nxp + x;
@@ -291,9 +299,9 @@ __device__ __forceinline__ void collide_shifted(const ChanF &k, float f[9], floa
             pull9s<S>(sf, pl, nxp, x, 1, xm, xp, 0, 2, m);
             reframe(m, __ldg(k.kref + 0) - kf1, __ldg(k.kref + 2) - kf1);
         }
-        const float rho1 = (float)(36.0 * kf1 + (double)sum9f(m));
-        ux = -(momx(m) * k.inv_cfl + fx * k.half_dt) / rho1;
-        uy = -(momy(m) * k.inv_cfl + fy * k.half_dt) / rho1;
+        const float rrho1 = 1.0f / (float)(36.0 * kf1 + (double)sum9f(m));
+        ux = -(momx(m) * k.inv_cfl + fx * k.half_dt) * rrho1;
+        uy = -(momy(m) * k.inv_cfl + fy * k.half_dt) * rrho1;
     }
     if (moments) {
         fields[F_RHO * pl + o] = Rf + (double)drho;
@@ -303,9 +311,9 @@ __device__ __forceinline__ void collide_shifted(const ChanF &k, float f[9], floa
         fields[F_CN * pl + o] = Rt + (double)dcn;
     }
     if (!lo && !hi) {
-        double v = -k.f_charge * qnet / k.eps;
-        if (y == 1) v = v - k.zlo[x] / k.dy / k.dy;
-        if (y == k.ny - 2) v = v - k.zhi[x] / k.dy / k.dy;
+        double v = k.rhs_q * qnet;
+        if (y == 1) v = v - k.zlo[x] * k.inv_dy2;
+        if (y == k.ny - 2) v = v - k.zhi[x] * k.inv_dy2;
         fields[F_RHS * pl + o] = v;
     }
     const float uxf = ux, uyf = uy;
@@ -381,7 +389,7 @@ __device__ __forceinline__ void init_node_shifted(const ChanF &k, S *__restrict_
         exd = fields[F_EX * pl + o];
         eyd = fields[F_EY * pl + o];
     } else {
-        efield_at_d(fields + F_PSI * pl, k.nxp, k.ny, k.dx, k.dy, x, y, xm, xp, &exd, &eyd);
+        efield_shifted(k, fields + F_PSI * pl, x, y, xm, xp, &exd, &eyd);
     }
     const float ux = (float)fields[F_UX * pl + o], uy = (float)fields[F_UY * pl + o];
     const float Ex = (float)exd, Ey = (float)eyd;

@@ -104,6 +104,8 @@ _SIGS = {
     "ek_batch_set_tile_width": ([ctypes.c_void_p, ctypes.c_int32], ctypes.c_int),
     "ek_batch_autotune": ([ctypes.c_void_p, ctypes.c_int32, _P(ctypes.c_int32), _dp], ctypes.c_int),
     "ek_batch_residual": ([ctypes.c_void_p, ctypes.c_int32, _dp, _dp], ctypes.c_int),
+    "ek_batch_set_active": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "ek_batch_active": ([ctypes.c_void_p, ctypes.c_void_p, _P(ctypes.c_int64)], ctypes.c_int),
     "ek_mlp_create": ([ctypes.c_int32, ctypes.c_uint64, _P(ctypes.c_void_p)], ctypes.c_int),
     "ek_mlp_destroy": ([ctypes.c_void_p], ctypes.c_int),
     "ek_mlp_param_count": ([ctypes.c_void_p, _P(ctypes.c_int64)], ctypes.c_int),

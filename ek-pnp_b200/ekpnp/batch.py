@@ -109,6 +109,20 @@ class Batch:
                                       ms.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
         return int(chosen.value), dict(zip((64, 128, 256), ms.tolist()))
 
+    def set_active(self, mask):
+        """Freeze (False) or step (True) each channel."""
+        m = np.ascontiguousarray(np.asarray(mask, dtype=bool).astype(np.uint8))
+        if m.shape != (len(self.channels),):
+            raise ValueError("one flag per channel")
+        check(lib().ek_batch_set_active(self._h, ctypes.c_void_p(m.ctypes.data)))
+
+    @property
+    def active(self):
+        m = np.zeros(len(self.channels), dtype=np.uint8)
+        n = ctypes.c_int64(0)
+        check(lib().ek_batch_active(self._h, ctypes.c_void_p(m.ctypes.data), ctypes.byref(n)))
+        return m.astype(bool), int(n.value)
+
     def residual(self, interval):
         """Per-channel residuals (n, 5): u_x, c+, c-, psi, max (inf before the first snapshot)."""
         out = np.zeros((len(self.channels), 5))

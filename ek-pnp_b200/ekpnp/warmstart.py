@@ -159,28 +159,41 @@ def physics_start(batch, specs):
         ch.set_fields(**profile_fields(s, physics_profiles(s), nx=ch.nx))
 
 
-def run_to_steady(batch, tol=1e-8, check=1000, max_steps=200_000, judge=None):
+def run_to_steady(batch, tol=1e-8, check=1000, max_steps=200_000, judge=None, freeze=True):
     """Step the batch until every channel has residual < tol (checked every
-    `check` steps) or diverged, or max_steps.  Returns per-channel steps to
+    `check` steps, an even number) or diverged, or max_steps.  With freeze,
+    channels stop stepping once converged or diverged (and, with judge, once
+    judged), so the work shrinks as they finish.  Returns per-channel steps to
     steady (-1: not reached), a diverged mask, the residual history (one row
-    per check) and the wall time in seconds (host clock, checks included).
-    judge=(k1, k2): also return the channels whose worst residual rose from
-    check k1 to check k2."""
+    per check; frozen channels repeat their last value) and the wall time in
+    seconds (host clock, checks included).  judge=(k1, k2): also return the
+    channels whose worst residual rose from check k1 to check k2."""
     n = len(batch)
     steps_to = np.full(n, -1, dtype=np.int64)
     hist = []
+    done = np.zeros(n, bool)
+    last = np.full(n, np.inf)
     batch.sync()
     t0 = time.perf_counter()
     batch.residual(check)  # first snapshot
     while batch.steps < max_steps:
         batch.step(min(check, max_steps - batch.steps))
         r = batch.residual(check)[:, 4]
+        r = np.where(done, last, r)
+        last = r
         hist.append(r)
         ok = np.isfinite(r)
         newly = (steps_to < 0) & ok & (r < tol)
         steps_to[newly] = batch.steps
         if np.all((steps_to >= 0) | ~ok):
             break
+        if freeze:
+            stop = (steps_to >= 0) | ~ok
+            if judge is not None and len(hist) > judge[1]:
+                stop |= rising_channels(np.array(hist), *judge)
+            if np.any(stop & ~done):
+                done |= stop
+                batch.set_active(~done)
     wall = time.perf_counter() - t0
     hist = np.array(hist)
     diverged = ~np.isfinite(hist[-1]) if len(hist) else np.zeros(n, bool)
@@ -238,14 +251,28 @@ class Surrogate:
         self.net.close()
 
     def _base(self, specs):
+        """Encoded physics start (zeros for "direct") and the per-channel factor
+        of the velocity block: the physics start's peak u_x / u_HS, so that the
+        velocity correction of a thick double layer (peak far below u_HS) is
+        learned relative to its own size."""
         if self.mode == "direct":
-            return np.zeros((len(specs), 4 * NS), dtype=np.float32)
-        return np.stack([encode(s, physics_profiles(s)) for s in specs])
+            return np.zeros((len(specs), 4 * NS), dtype=np.float32), np.ones(len(specs), dtype=np.float32)
+        base = np.stack([encode(s, physics_profiles(s)) for s in specs])
+        peak = np.maximum(base[:, 3 * NS:].max(axis=1), 1e-3).astype(np.float32)
+        return base, peak
+
+    def _unscale(self, specs, y):
+        base, peak = self._base(specs)
+        y = y.copy()
+        y[:, 3 * NS:] *= peak[:, None]
+        return base + y
 
     def fit(self, specs, targets, iters=8000, lr=2e-3, chunks=8):
         """Adam with a cosine learning-rate decay in `chunks` steps; returns the
         per-iteration losses (of the scaled targets)."""
-        y = targets - self._base(specs)
+        base, peak = self._base(specs)
+        y = targets - base
+        y[:, 3 * NS:] /= peak[:, None]
         self.offset = y.mean(axis=0).astype(np.float32)
         self.scale = np.maximum(y.std(axis=0), 1e-6).astype(np.float32)
         self.net.set_data(features(specs), (y - self.offset) / self.scale)
@@ -257,7 +284,7 @@ class Surrogate:
         return np.concatenate(losses)
 
     def predict(self, specs):
-        return self._base(specs) + self.net.forward(features(specs)) * self.scale + self.offset
+        return self._unscale(specs, self.net.forward(features(specs)) * self.scale + self.offset)
 
     def fields(self, specs):
         return [decode(s, v) for s, v in zip(specs, self.predict(specs))]

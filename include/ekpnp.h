@@ -293,6 +293,14 @@ int ek_batch_set_tile_width(ek_batch *b, int32_t width);
  * 3 (steps + 2) steps), keeps the fastest; ms3 (optional): ms per step of
  * widths 64, 128, 256. */
 int ek_batch_autotune(ek_batch *b, int32_t steps, int32_t *chosen, double *ms3);
+/* Freeze (mask[i] == 0) or step (mask[i] != 0) each channel; a frozen
+ * channel keeps its state and step count, the launches per step stay four
+ * and the work shrinks to the active channels (a run to steady state freezes
+ * the channels that have converged).  A frozen channel rejoins only after an
+ * even number of batch steps.  ek_batch_init_equilibrium activates all. */
+int ek_batch_set_active(ek_batch *b, const uint8_t *mask);
+/* mask (optional, count bytes) and the number of active nodes (optional). */
+int ek_batch_active(const ek_batch *b, uint8_t *mask, int64_t *active_nodes);
 /* ek_residual of every channel: out5 gets 5 doubles per channel (u_x, c+,
  * c-, psi, max), worst5 (optional) the maxima over the finite channels.  A
  * channel holding non-finite values gets NaN residuals (the call succeeds). */

@@ -176,3 +176,33 @@ def test_unsupported_channels_are_rejected():
             ekpnp.Batch([dict(p, **bad)])
     with pytest.raises(ekpnp.EkError):
         ekpnp.Batch([p, dict(p, storage=ekpnp.STORE_F16)])
+
+
+def test_frozen_channels_keep_their_state_and_others_keep_the_bits():
+    import ekpnp
+    ps, ins = params(ekpnp.STORE_F32), inits()
+    with ekpnp.Batch(ps) as b:
+        for ch, init in zip(b, ins):
+            ch.set_fields(**init)
+        b.set_cycle(10)
+        b.init_equilibrium()
+        b.step(10)
+        mask = np.ones(len(ps), bool)
+        mask[[1, 4]] = False
+        b.set_active(mask)
+        active, nodes = b.active
+        assert active.tolist() == mask.tolist()
+        assert nodes == sum(s["nx"] * s["ny"] for s, m in zip(SPECS, mask) if m)
+        frozen = {i: b[i].get_fields(NAMES) for i in (1, 4)}
+        b.step(27)
+        with pytest.raises(ekpnp.EkError):   # 27 steps later the parity differs
+            b.set_active(np.ones(len(ps), bool))
+        for i in range(len(ps)):
+            got = b[i].get_fields(NAMES)
+            ref = frozen[i] if i in frozen else single(ps[i], ins[i], 37, 10)
+            for k in NAMES:
+                assert np.array_equal(got[k], ref[k]), (i, k)
+        b.step(1)
+        b.set_active(np.ones(len(ps), bool))  # even now: rejoin allowed
+        b.step(2)
+        assert all(np.all(np.isfinite(ch.get_fields(("ux",))["ux"])) for ch in b)
