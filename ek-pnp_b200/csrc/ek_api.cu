@@ -87,6 +87,9 @@ void free_ctx(ek_ctx *c) {
     cudaFree(c->pp.tw);
     cudaFree(c->pp.piv);
     cudaFree(c->pp.spec);
+    cudaFree(c->pp.twf);
+    cudaFree(c->pp.pivf);
+    cudaFree(c->pp.specf);
     for (auto &pr : c->ev_pool) {
         cudaEventDestroy(pr.first);
         cudaEventDestroy(pr.second);
@@ -256,8 +259,12 @@ int timed(ek_ctx *c, int phase, const char *what, Fn fn) {
 
 int poisson_now(ek_ctx *c) {
     for (int pass = 0; pass < 3; ++pass) {
-        int rc = timed(c, 1 + pass, "poisson kernel",
-                       [&] { return poisson_pass_f64(pass, c->pp, c->chan, c->fields, c->stream); });
+        const bool f32 = ek::ctx_poisson_f32(c);
+        int rc = timed(c, 1 + pass, "poisson kernel", [&] {
+            return f32 ? poisson_pass_f32_at(pass, c->pp, c->chan, c->fields + F_RHS * c->plane,
+                                             c->fields + F_PSI * c->plane, c->stream)
+                       : poisson_pass_f64(pass, c->pp, c->chan, c->fields, c->stream);
+        });
         if (rc != EK_OK) return rc;
     }
     if (c->p.flags & EK_FLAG_EXPLICIT_E) {
@@ -318,6 +325,10 @@ void set_last_error(const char *msg) { g_err = msg; }
 int ctx_fail(int code, const char *msg) { return fail(code, msg); }
 int ctx_refs_from_fields(ek_ctx *c, float *out) { return refs_from_fields(c, out); }
 void ctx_refresh(ek_ctx *c) { refresh_chan(c); }
+bool ctx_poisson_f32(const ek_ctx *c) {
+    if (c->poisson_mode == 1 || c->p.storage == EK_STORE_F64) return false;
+    return poisson_f32_supported(c->pp);
+}
 
 int ctx_residual_buffers(ek_ctx *c) {
     if (c->snap) return EK_OK;
@@ -484,6 +495,23 @@ int ek_create(const ek_params *p, ek_ctx **out) {
     while ((1 << lg) < p->nx) ++lg;
     c->pp.log2nx = c->pp.pow2 ? lg : 0;
     c->pp.dy2 = p->dy * p->dy;
+    if (p->storage != EK_STORE_F64 && c->pp.pow2 && p->nx >= 16 && poisson_tridiag_modes(c->n) > 0) {
+        // FP32 form of the Poisson solve: FP32 twiddles, pivots and spectrum
+        std::vector<float> pivf(piv.begin(), piv.end());
+        std::vector<float2> twf(tw.size());
+        for (size_t i = 0; i < tw.size(); ++i) twf[i] = make_float2((float)tw[i].x, (float)tw[i].y);
+        e = cudaMalloc(&c->pp.twf, twf.size() * sizeof(float2));
+        if (e == cudaSuccess) e = cudaMalloc(&c->pp.pivf, pivf.size() * sizeof(float));
+        if (e == cudaSuccess) e = cudaMalloc(&c->pp.specf, (size_t)c->n * c->mp * sizeof(float2));
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->pp.specf, 0, (size_t)c->n * c->mp * sizeof(float2), c->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(c->pp.twf, twf.data(), twf.size() * sizeof(float2), cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(c->pp.pivf, pivf.data(), pivf.size() * sizeof(float), cudaMemcpyHostToDevice,
+                                c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) { free_ctx(c); return cuda_fail(e, "FP32 Poisson set-up"); }
+    }
     refresh_chan(c);
     *out = c;
     return EK_OK;
@@ -751,6 +779,14 @@ int ek_set_option(ek_ctx *c, int32_t option, int64_t value) {
         if (value == 2 && !(shifted(c) && c->tma_ok))
             return fail(EK_ERR_UNSUPPORTED, "TMA-fed kernel needs shifted storage and a tensor map");
         c->lbm_kernel = (int)value;
+        return EK_OK;
+    }
+    if (option == EK_OPT_POISSON) {
+        if (value < 0 || value > 2) return fail(EK_ERR_INVALID, "EK_OPT_POISSON takes 0, 1 or 2");
+        if (value == 2 && !poisson_f32_supported(c->pp))
+            return fail(EK_ERR_UNSUPPORTED, "the FP32 Poisson form needs shifted storage, a power-of-two nx >= 16 "
+                                            "and ny <= 8194");
+        c->poisson_mode = (int)value;
         return EK_OK;
     }
     return fail(EK_ERR_INVALID, "unknown option");

@@ -177,6 +177,7 @@ struct ek_batch {
     int cycle = 200;                 // steps per cycle (even)
     bool rebase = true;
     bool use_graph = true;
+    bool poisson_f32 = false;        // every channel runs the FP32 Poisson form
     cudaGraphExec_t graph = nullptr;
     int graph_cur = -1;              // parity the graph was captured for
     int64_t launches = 0;
@@ -273,6 +274,9 @@ int build_tables(ek_batch *b) {
     release_graph(b);
     b->kcur.clear();
     int nrpart = 0;
+    bool f32 = true;
+    for (ek_ctx *c : b->ch) f32 = f32 && ek::ctx_poisson_f32(c);
+    b->poisson_f32 = f32;
     for (size_t i = 0; i < b->ch.size(); ++i) {
         ek_ctx *c = b->ch[i];
         ek::ctx_refresh(c);
@@ -293,7 +297,11 @@ int build_tables(ek_batch *b) {
             const int per = 256 / (nx >> 4);
             for (int q = 0; q < (n + 1) / 2; q += per) pairs.push_back(make_int2((int)i, q));
             const int M = poisson_tridiag_modes(n);
-            for (int m0 = 0; m0 <= nx / 2; m0 += M) modes.push_back(make_int3((int)i, m0, M));
+            if (f32) {  // block 0: the FP64 zero mode; blocks 1..: modes 1.. in FP32
+                for (int blk = 0; blk <= (nx / 2 + M - 1) / M; ++blk) modes.push_back(make_int3((int)i, blk, M));
+            } else {
+                for (int m0 = 0; m0 <= nx / 2; m0 += M) modes.push_back(make_int3((int)i, m0, M));
+            }
             for (int y = 0; y < c->p.ny; ++y) rows.push_back(make_int2((int)i, y));
         }
         const int nb = residual_blocks(c->chan);
@@ -337,9 +345,9 @@ int launch_step(ek_batch *b, bool first, bool ee, bool mom) {
                         : lbm_s<float>(b->txb, b->d_chanf, src, dst, b->d_fields, b->d_tiles, b->ntiles, b->grid,
                                        first, ee, mom, b->stream);
     EK_BCUDA(e, "batch LBM kernel");
-    EK_BCUDA(batch_poisson(0, b->d_plans, b->d_chan, b->d_fields, b->d_pairs, b->npairs, b->stream), "batch rows");
-    EK_BCUDA(batch_poisson(1, b->d_plans, b->d_chan, b->d_fields, b->d_modes, b->nmodes, b->stream), "batch modes");
-    EK_BCUDA(batch_poisson(2, b->d_plans, b->d_chan, b->d_fields, b->d_pairs, b->npairs, b->stream), "batch rows");
+    EK_BCUDA(batch_poisson(0, b->d_plans, b->d_chan, b->d_fields, b->d_pairs, b->npairs, b->stream, b->poisson_f32), "batch rows");
+    EK_BCUDA(batch_poisson(1, b->d_plans, b->d_chan, b->d_fields, b->d_modes, b->nmodes, b->stream, b->poisson_f32), "batch modes");
+    EK_BCUDA(batch_poisson(2, b->d_plans, b->d_chan, b->d_fields, b->d_pairs, b->npairs, b->stream, b->poisson_f32), "batch rows");
     b->launches += 4;
     b->cur ^= 1;
     return EK_OK;

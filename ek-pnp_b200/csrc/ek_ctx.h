@@ -35,6 +35,7 @@ struct ek_ctx {
     CUtensorMap tmaps[2];                 // shifted storage: TMA descriptors of pops[0], pops[1]
     bool tma_ok = false;
     int lbm_kernel = 0;                   // EK_OPT_LBM_KERNEL
+    int poisson_mode = 0;                 // EK_OPT_POISSON
     int *err_dev = nullptr;               // set by bounded device waits
     ek::Rates *rates_dev = nullptr;
     ek::Rates rates{};
@@ -57,4 +58,5 @@ int ctx_refs_from_fields(ek_ctx *c, float *out);
 void ctx_refresh(ek_ctx *c);
 int ctx_residual_buffers(ek_ctx *c);
 int ctx_residual_finish(ek_ctx *c, const double *sums, int32_t interval, double *out5);
+bool ctx_poisson_f32(const ek_ctx *c);  // the FP32 form runs for this context
 }  // namespace ek

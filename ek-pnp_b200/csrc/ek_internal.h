@@ -101,6 +101,11 @@ struct PoissonPlan {
     double2 *tw;                // nx twiddles exp(-2 pi i k/nx)
     double *piv;                // n x mp pivots
     double2 *spec;              // n x mp spectrum
+    // FP32 form (shifted storage): modes >= 1 in FP32, the zero mode in FP64
+    // (column 0 of spec); null where the form is not set up
+    float2 *twf;                // nx twiddles, FP32
+    float *pivf;                // n x mp pivots, FP32
+    float2 *specf;              // n x mp spectrum, FP32
 };
 // pass 0: row FFTs, 1: tridiagonal column solve, 2: inverse row FFTs + walls
 cudaError_t poisson_pass_f64(int pass, const PoissonPlan &pp, const Chan &c, double *fields, cudaStream_t s);
@@ -108,12 +113,19 @@ cudaError_t poisson_pass_f64(int pass, const PoissonPlan &pp, const Chan &c, dou
 cudaError_t poisson_pass_f64_at(int pass, const PoissonPlan &pp, const Chan &c, const double *rhs, double *psi,
                                 cudaStream_t s);
 size_t poisson_smem_bytes_f64(int nx);
+// FP32 form of the passes (power-of-two nx >= 16, n <= 8192, twf/pivf/specf
+// set): the row FFTs and the column solves of the modes >= 1 in FP32 on the
+// fluctuation about each row's mean; the row sums (the zero mode), its
+// column solve and the mean of psi in FP64.
+bool poisson_f32_supported(const PoissonPlan &pp);
+cudaError_t poisson_pass_f32_at(int pass, const PoissonPlan &pp, const Chan &c, const double *rhs, double *psi,
+                                cudaStream_t s);
 // Batched Poisson passes over many channels (ek_batch.cu builds the items):
 // pass 0/2 items int2 {channel, first row pair} (256-thread blocks, each
 // 256/(nx/16) row pairs; power-of-two nx from 16 to 4096); pass 1 items
 // int3 {channel, first mode, modes per block}.
 cudaError_t batch_poisson(int pass, const PoissonPlan *plans, const Chan *chans, double *const *fields,
-                          const void *items, int nitems, cudaStream_t s);
+                          const void *items, int nitems, cudaStream_t s, bool f32 = false);
 int poisson_tridiag_modes(int n);
 // Steady-state residual sums (ek_residual.cu): per channel 8 FP64 sums,
 // (q - q_snap)^2 then q^2 for q in (ux, c+, c-, psi); the snapshot is updated.

@@ -33,6 +33,15 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+template <typename C> __device__ __forceinline__ C cmake(double a, double b);
+template <> __device__ __forceinline__ double2 cmake<double2>(double a, double b) { return make_double2(a, b); }
+template <> __device__ __forceinline__ float2 cmake<float2>(double a, double b) { return make_float2((float)a, (float)b); }
 
 // In-place radix-2 decimation-in-time FFT of n = 2^lg points already in
 // bit-reversed order in shared memory.  inv selects the +i exponent.
@@ -197,22 +206,23 @@ __device__ __forceinline__ int swz(int i, int k) {
 }
 
 // exp(-2 pi i v/2^(sl+1)) for 0 <= v < 2^sl <= 8 (compile-time arguments)
-__device__ __forceinline__ double2 root16(int sl, int v) {
+template <typename C>
+__device__ __forceinline__ C root16(int sl, int v) {
     const int q = v << (3 - sl);  // angle = q * pi/8
     switch (q) {
-        case 0: return make_double2(1.0, 0.0);
-        case 1: return make_double2(0.92387953251128674, -0.38268343236508977);
-        case 2: return make_double2(0.70710678118654752, -0.70710678118654752);
-        case 3: return make_double2(0.38268343236508977, -0.92387953251128674);
-        case 4: return make_double2(0.0, -1.0);
-        case 5: return make_double2(-0.38268343236508977, -0.92387953251128674);
-        case 6: return make_double2(-0.70710678118654752, -0.70710678118654752);
-        default: return make_double2(-0.92387953251128674, -0.38268343236508977);
+        case 0: return cmake<C>(1.0, 0.0);
+        case 1: return cmake<C>(0.92387953251128674, -0.38268343236508977);
+        case 2: return cmake<C>(0.70710678118654752, -0.70710678118654752);
+        case 3: return cmake<C>(0.38268343236508977, -0.92387953251128674);
+        case 4: return cmake<C>(0.0, -1.0);
+        case 5: return cmake<C>(-0.38268343236508977, -0.92387953251128674);
+        case 6: return cmake<C>(-0.70710678118654752, -0.70710678118654752);
+        default: return cmake<C>(-0.92387953251128674, -0.38268343236508977);
     }
 }
 
-template <bool INV, int RB>
-__device__ __forceinline__ void reg_pass(double2 *s, int k, int T, int t, int b, const double2 *__restrict__ tw) {
+template <bool INV, int RB, typename C>
+__device__ __forceinline__ void reg_pass(C *s, int k, int T, int t, int b, const C *__restrict__ tw) {
     constexpr int G = 16 >> RB, E = 1 << RB;
     const int ngroups = (1 << k) >> RB;
 #pragma unroll
@@ -221,19 +231,19 @@ __device__ __forceinline__ void reg_pass(double2 *s, int k, int T, int t, int b,
         if (g >= ngroups) continue;
         const int kb = g & ((1 << b) - 1);
         const int base = kb | ((g >> b) << (b + RB));
-        double2 r[E];
+        C r[E];
 #pragma unroll
         for (int v = 0; v < E; ++v) r[v] = s[swz(base | (v << b), k)];
         if (!INV) {
 #pragma unroll
             for (int sl = RB - 1; sl >= 0; --sl) {
                 const int st = b + sl;
-                const double2 A = __ldg(tw + (kb << (k - st - 1)));
+                const C A = __ldg(tw + (kb << (k - st - 1)));
 #pragma unroll
                 for (int v = 0; v < E; ++v) {
                     if (v & (1 << sl)) continue;
-                    const double2 w = cmul(A, root16(sl, v & ((1 << sl) - 1)));
-                    const double2 u = r[v], x = r[v + (1 << sl)];
+                    const C w = cmul(A, root16<C>(sl, v & ((1 << sl) - 1)));
+                    const C u = r[v], x = r[v + (1 << sl)];
                     r[v] = cadd(u, x);
                     r[v + (1 << sl)] = cmul(csub(u, x), w);
                 }
@@ -242,12 +252,12 @@ __device__ __forceinline__ void reg_pass(double2 *s, int k, int T, int t, int b,
 #pragma unroll
             for (int sl = 0; sl < RB; ++sl) {
                 const int st = b + sl;
-                const double2 A = cconj(__ldg(tw + (kb << (k - st - 1))));
+                const C A = cconj(__ldg(tw + (kb << (k - st - 1))));
 #pragma unroll
                 for (int v = 0; v < E; ++v) {
                     if (v & (1 << sl)) continue;
-                    const double2 w = cmul(A, cconj(root16(sl, v & ((1 << sl) - 1))));
-                    const double2 u = r[v], x = cmul(r[v + (1 << sl)], w);
+                    const C w = cmul(A, cconj(root16<C>(sl, v & ((1 << sl) - 1))));
+                    const C u = r[v], x = cmul(r[v + (1 << sl)], w);
                     r[v] = cadd(u, x);
                     r[v + (1 << sl)] = csub(u, x);
                 }
@@ -258,30 +268,30 @@ __device__ __forceinline__ void reg_pass(double2 *s, int k, int T, int t, int b,
     }
 }
 
-template <bool INV>
-__device__ __forceinline__ void reg_pass_any(double2 *s, int k, int T, int t, int b, int rb, const double2 *tw) {
+template <bool INV, typename C>
+__device__ __forceinline__ void reg_pass_any(C *s, int k, int T, int t, int b, int rb, const C *tw) {
     switch (rb) {
-        case 4: reg_pass<INV, 4>(s, k, T, t, b, tw); break;
-        case 3: reg_pass<INV, 3>(s, k, T, t, b, tw); break;
-        case 2: reg_pass<INV, 2>(s, k, T, t, b, tw); break;
-        default: reg_pass<INV, 1>(s, k, T, t, b, tw); break;
+        case 4: reg_pass<INV, 4, C>(s, k, T, t, b, tw); break;
+        case 3: reg_pass<INV, 3, C>(s, k, T, t, b, tw); break;
+        case 2: reg_pass<INV, 2, C>(s, k, T, t, b, tw); break;
+        default: reg_pass<INV, 1, C>(s, k, T, t, b, tw); break;
     }
 }
 
 // Whole transform of 2^k points in s; every thread of the block calls it.
-template <bool INV>
-__device__ void reg_fft(double2 *s, int k, int T, int t, const double2 *__restrict__ tw) {
+template <bool INV, typename C>
+__device__ void reg_fft(C *s, int k, int T, int t, const C *__restrict__ tw) {
     if (!INV) {
         for (int top = k; top > 0;) {
             const int rb = top < 4 ? top : 4;
-            reg_pass_any<false>(s, k, T, t, top - rb, rb, tw);
+            reg_pass_any<false, C>(s, k, T, t, top - rb, rb, tw);
             __syncthreads();
             top -= rb;
         }
     } else {
         for (int b = 0; b < k;) {
             const int rb = k - b < 4 ? k - b : 4;
-            reg_pass_any<true>(s, k, T, t, b, rb, tw);
+            reg_pass_any<true, C>(s, k, T, t, b, rb, tw);
             __syncthreads();
             b += rb;
         }
@@ -303,7 +313,7 @@ __device__ __forceinline__ void fwd_rows_r16_dev(const PoissonPlan &pp, const do
     for (int x = t; x < N; x += T)
         s[swz(x, k)] = live ? make_double2(__ldg(r0 + x), two ? __ldg(r1 + x) : 0.0) : make_double2(0.0, 0.0);
     __syncthreads();
-    reg_fft<false>(s, k, T, t, pp.tw);
+    reg_fft<false, double2>(s, k, T, t, pp.tw);
     if (!live) return;
     double2 *s0 = pp.spec + (size_t)j0 * pp.mp, *s1 = pp.spec + (size_t)j1 * pp.mp;
     for (int m = t; m <= N / 2; m += T) {
@@ -340,7 +350,7 @@ __device__ __forceinline__ void inv_rows_r16_dev(const PoissonPlan &pp, int nxp,
         if (m != 0 && 2 * m != N) s[swz(brev(N - m, k), k)] = make_double2(a.x + b.y, -a.y + b.x);
     }
     __syncthreads();
-    reg_fft<true>(s, k, T, t, pp.tw);
+    reg_fft<true, double2>(s, k, T, t, pp.tw);
     const double inv = 1.0 / (double)N;
     if (live) {
         double *p0 = psi + (size_t)(j0 + 1) * nxp, *p1 = psi + (size_t)(j1 + 1) * nxp;
@@ -366,6 +376,125 @@ inv_rows_r16(const PoissonPlan pp, const Chan c, double *__restrict__ psi) {
     inv_rows_r16_dev<BLOCK>(pp, c.nxp, c.ny, c.zlo, c.zhi, psi, blockIdx.x * (BLOCK / (pp.nx >> 4)), sm);
 }
 
+// ---- FP32 form of passes A and C ------------------------------------------
+// The row is split into its mean (FP64: the zero mode) and the fluctuation
+// about it, which is transformed in FP32.  The zero mode of every row is
+// kept in column 0 of the FP64 spectrum; modes 1..nx/2 go to the FP32
+// spectrum.
+
+// Sum of v over the T threads of one transform group (T a power of two,
+// groups contiguous in the block); every thread of the block calls it and
+// gets the group's first lane's (or the block-level) value.
+template <int BLOCK>
+__device__ __forceinline__ double group_sum(double v, int T, double *red) {
+    const int w = T < 32 ? T : 32;
+    for (int o = w >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (T < 32) return __shfl_sync(0xffffffffu, v, (threadIdx.x & 31) & ~(T - 1));
+    v = __shfl_sync(0xffffffffu, v, 0);
+    if (T == 32) return v;
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    const int nw = T >> 5, g0 = (int)(threadIdx.x / T) * nw;
+    double s = 0.0;
+    for (int i = 0; i < nw; ++i) s += red[g0 + i];
+    __syncthreads();
+    return s;
+}
+
+template <int BLOCK>
+__device__ __forceinline__ void fwd_rows_r16f_dev(const PoissonPlan &pp, const double *__restrict__ rhs, int nxp,
+                                                  int pair_base, float2 *sm, double *red) {
+    const int N = pp.nx, k = pp.log2nx, T = N >> 4;
+    const int p = threadIdx.x / T, t = threadIdx.x - p * T;
+    const int pair = pair_base + p;
+    float2 *s = sm + p * N;
+    const int j0 = 2 * pair, j1 = j0 + 1;
+    const bool live = j0 < pp.n, two = j1 < pp.n;
+    const double *r0 = rhs + (size_t)(j0 + 1) * nxp, *r1 = rhs + (size_t)(j1 + 1) * nxp;
+    double a0 = 0.0, a1 = 0.0;
+    for (int x = t; x < N; x += T) {
+        if (live) a0 += __ldg(r0 + x);
+        if (two) a1 += __ldg(r1 + x);
+    }
+    a0 = group_sum<BLOCK>(a0, T, red);
+    a1 = group_sum<BLOCK>(a1, T, red);
+    if (t == 0 && live) {
+        pp.spec[(size_t)j0 * pp.mp] = make_double2(a0, 0.0);
+        if (two) pp.spec[(size_t)j1 * pp.mp] = make_double2(a1, 0.0);
+    }
+    const double m0 = a0 / (double)N, m1 = a1 / (double)N;
+    for (int x = t; x < N; x += T)
+        s[swz(x, k)] = live ? make_float2((float)(__ldg(r0 + x) - m0), two ? (float)(__ldg(r1 + x) - m1) : 0.0f)
+                            : make_float2(0.0f, 0.0f);
+    __syncthreads();
+    reg_fft<false, float2>(s, k, T, t, pp.twf);
+    if (!live) return;
+    float2 *s0 = pp.specf + (size_t)j0 * pp.mp, *s1 = pp.specf + (size_t)j1 * pp.mp;
+    for (int m = t; m <= N / 2; m += T) {
+        if (m == 0) continue;
+        const float2 a = s[swz(brev(m, k), k)], b = cconj(s[swz(brev(N - m, k), k)]);
+        s0[m] = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y + b.y));
+        if (two) s1[m] = make_float2(0.5f * (a.y - b.y), -0.5f * (a.x - b.x));
+    }
+}
+
+template <int BLOCK>
+__device__ __forceinline__ void inv_rows_r16f_dev(const PoissonPlan &pp, int nxp, int ny, const double *zlo,
+                                                  const double *zhi, double *__restrict__ psi, int pair_base,
+                                                  float2 *sm) {
+    const int N = pp.nx, k = pp.log2nx, T = N >> 4;
+    const int p = threadIdx.x / T, t = threadIdx.x - p * T;
+    const int pair = pair_base + p;
+    float2 *s = sm + p * N;
+    const int j0 = 2 * pair, j1 = j0 + 1;
+    const bool live = j0 < pp.n, two = j1 < pp.n;
+    const float2 *s0 = pp.specf + (size_t)j0 * pp.mp, *s1 = pp.specf + (size_t)j1 * pp.mp;
+    for (int m = t; m <= N / 2; m += T) {
+        const float2 a = (live && m) ? s0[m] : make_float2(0.0f, 0.0f);
+        const float2 b = (two && m) ? s1[m] : make_float2(0.0f, 0.0f);
+        s[swz(brev(m, k), k)] = make_float2(a.x - b.y, a.y + b.x);  // A + iB
+        if (m != 0 && 2 * m != N) s[swz(brev(N - m, k), k)] = make_float2(a.x + b.y, -a.y + b.x);
+    }
+    __syncthreads();
+    reg_fft<true, float2>(s, k, T, t, pp.twf);
+    const double inv = 1.0 / (double)N;
+    if (live) {
+        const double mean0 = pp.spec[(size_t)j0 * pp.mp].x * inv;
+        const double mean1 = two ? pp.spec[(size_t)j1 * pp.mp].x * inv : 0.0;
+        double *p0 = psi + (size_t)(j0 + 1) * nxp, *p1 = psi + (size_t)(j1 + 1) * nxp;
+        for (int x = t; x < N; x += T) {
+            const float2 z = s[swz(x, k)];
+            p0[x] = mean0 + (double)z.x * inv;
+            if (two) p1[x] = mean1 + (double)z.y * inv;
+        }
+    }
+    if (pair_base == 0) {
+        double *lo = psi, *hi = psi + (size_t)(ny - 1) * nxp;
+        for (int x = threadIdx.x; x < N; x += BLOCK) {
+            lo[x] = zlo[x];
+            hi[x] = zhi[x];
+        }
+    }
+}
+
+// 4 blocks of 256 threads per SM: the 511 row pairs of a 4096 x 1024 channel
+// then run in one wave (3 blocks per SM leave a second, nearly empty wave).
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
+fwd_rows_r16f(const PoissonPlan pp, const double *__restrict__ rhs, int nxp) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ double red[BLOCK / 32];
+    fwd_rows_r16f_dev<BLOCK>(pp, rhs, nxp, blockIdx.x * (BLOCK / (pp.nx >> 4)), (float2 *)smraw, red);
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
+inv_rows_r16f(const PoissonPlan pp, const Chan c, double *__restrict__ psi) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    inv_rows_r16f_dev<BLOCK>(pp, c.nxp, c.ny, c.zlo, c.zhi, psi, blockIdx.x * (BLOCK / (pp.nx >> 4)),
+                             (float2 *)smraw);
+}
+
 // ---- pass B, partitioned Thomas solve ------------------------------------
 //
 // A block owns M consecutive x-modes; its 512 threads are S = 512/M row
@@ -380,37 +509,39 @@ inv_rows_r16(const PoissonPlan pp, const Chan c, double *__restrict__ psi) {
 constexpr int TB_THREADS = 512;
 constexpr int TB_L = 16;
 
-struct TridiagShared {
-    double2 ends[TB_THREADS];
-    double mults[TB_THREADS];
-    double2 carry[TB_THREADS];
+template <typename R, typename C> struct TridiagSharedT {
+    C ends[TB_THREADS];
+    R mults[TB_THREADS];
+    C carry[TB_THREADS];
 };
+using TridiagShared = TridiagSharedT<double, double2>;
 
-__device__ __forceinline__ void tridiag_part_dev(const PoissonPlan &pp, int M, int m_base, TridiagShared &sh) {
-    double2 *ends = sh.ends, *carry = sh.carry;
-    double *mults = sh.mults;
-    const int n = pp.n, mlast = pp.nx / 2;
-    const size_t mp = pp.mp;
+// One block of the partitioned solve on a spectrum of type C (pivots R).
+template <typename R, typename C>
+__device__ __forceinline__ void tridiag_part_gen(const R *__restrict__ piv, C *__restrict__ spec, int n, int nx,
+                                                 size_t mp, R dy2, int M, int m_base, TridiagSharedT<R, C> &sh) {
+    C *ends = sh.ends, *carry = sh.carry;
+    R *mults = sh.mults;
+    const int mlast = nx / 2;
     const int tid = threadIdx.x, mode = tid % M, seg = tid / M, S = TB_THREADS / M;
     const int m = m_base + mode;
     const bool mvalid = m <= mlast;
     const int L = (n + S - 1) / S, ja = seg * L, cnt = max(0, min(n, ja + L) - ja);
-    double c[TB_L];
-    double2 v[TB_L];
-    const double dy2 = pp.dy2;
+    R c[TB_L];
+    C v[TB_L];
 #pragma unroll
     for (int q = 0; q < TB_L; ++q) {
         const bool on = mvalid && q < cnt;
-        c[q] = on ? __ldg(pp.piv + (size_t)(ja + q) * mp + m) : 0.0;
-        const double2 sv = on ? pp.spec[(size_t)(ja + q) * mp + m] : make_double2(0.0, 0.0);
-        v[q] = make_double2(dy2 * sv.x, dy2 * sv.y);
+        c[q] = on ? __ldg(piv + (size_t)(ja + q) * mp + m) : R(0);
+        const C sv = on ? spec[(size_t)(ja + q) * mp + m] : cmake<C>(0.0, 0.0);
+        v[q] = cmake<C>(dy2 * sv.x, dy2 * sv.y);
     }
-    double2 d = make_double2(0.0, 0.0);
-    double mu = 1.0;
+    C d = cmake<C>(0.0, 0.0);
+    R mu = R(1);
 #pragma unroll
     for (int q = 0; q < TB_L; ++q) {
         if (q < cnt) {
-            d = make_double2((v[q].x - d.x) * c[q], (v[q].y - d.y) * c[q]);
+            d = cmake<C>((v[q].x - d.x) * c[q], (v[q].y - d.y) * c[q]);
             mu = -c[q] * mu;
             v[q] = d;
         }
@@ -419,18 +550,18 @@ __device__ __forceinline__ void tridiag_part_dev(const PoissonPlan &pp, int M, i
     mults[tid] = mu;
     __syncthreads();
     if (seg == 0) {  // true entry value of every segment
-        double2 D = make_double2(0.0, 0.0);
+        C D = cmake<C>(0.0, 0.0);
         for (int s_ = 0; s_ < S; ++s_) {
             carry[s_ * M + mode] = D;
-            const double2 e = ends[s_ * M + mode];
-            const double f = mults[s_ * M + mode];
-            D = make_double2(e.x + f * D.x, e.y + f * D.y);
+            const C e = ends[s_ * M + mode];
+            const R f = mults[s_ * M + mode];
+            D = cmake<C>(e.x + f * D.x, e.y + f * D.y);
         }
     }
     __syncthreads();
     {
-        const double2 D = carry[tid];
-        mu = 1.0;
+        const C D = carry[tid];
+        mu = R(1);
 #pragma unroll
         for (int q = 0; q < TB_L; ++q) {
             if (q < cnt) {
@@ -440,12 +571,12 @@ __device__ __forceinline__ void tridiag_part_dev(const PoissonPlan &pp, int M, i
             }
         }
     }
-    double2 x = make_double2(0.0, 0.0);
-    double nu = 1.0;
+    C x = cmake<C>(0.0, 0.0);
+    R nu = R(1);
 #pragma unroll
     for (int q = TB_L - 1; q >= 0; --q) {
         if (q < cnt) {
-            x = make_double2(v[q].x - c[q] * x.x, v[q].y - c[q] * x.y);
+            x = cmake<C>(v[q].x - c[q] * x.x, v[q].y - c[q] * x.y);
             nu = -c[q] * nu;
             v[q] = x;
         }
@@ -455,30 +586,55 @@ __device__ __forceinline__ void tridiag_part_dev(const PoissonPlan &pp, int M, i
     mults[tid] = nu;
     __syncthreads();
     if (seg == 0) {  // true exit value of every segment (x_n = 0)
-        double2 X = make_double2(0.0, 0.0);
+        C X = cmake<C>(0.0, 0.0);
         for (int s_ = S - 1; s_ >= 0; --s_) {
             carry[s_ * M + mode] = X;
-            const double2 e = ends[s_ * M + mode];
-            const double f = mults[s_ * M + mode];
-            X = make_double2(e.x + f * X.x, e.y + f * X.y);
+            const C e = ends[s_ * M + mode];
+            const R f = mults[s_ * M + mode];
+            X = cmake<C>(e.x + f * X.x, e.y + f * X.y);
         }
     }
     __syncthreads();
     if (!mvalid) return;
-    const double2 X = carry[tid];
-    nu = 1.0;
+    const C X = carry[tid];
+    nu = R(1);
 #pragma unroll
     for (int q = TB_L - 1; q >= 0; --q) {
         if (q < cnt) {
             nu = -c[q] * nu;
-            pp.spec[(size_t)(ja + q) * mp + m] = make_double2(v[q].x + nu * X.x, v[q].y + nu * X.y);
+            spec[(size_t)(ja + q) * mp + m] = cmake<C>(v[q].x + nu * X.x, v[q].y + nu * X.y);
         }
     }
+}
+
+__device__ __forceinline__ void tridiag_part_dev(const PoissonPlan &pp, int M, int m_base, TridiagShared &sh) {
+    tridiag_part_gen<double, double2>(pp.piv, pp.spec, pp.n, pp.nx, (size_t)pp.mp, pp.dy2, M, m_base, sh);
+}
+
+// FP32 form of pass B: block 0 solves the zero mode in FP64 (the FP64
+// spectrum's column 0, with its neighbours up to M-1 solved alongside and
+// unused); blocks 1.. solve modes 1..nx/2 in FP32, M per block.
+__device__ __forceinline__ void tridiag_part_f32_dev(const PoissonPlan &pp, int M, int block) {
+    __shared__ union {
+        TridiagSharedT<double, double2> d;
+        TridiagSharedT<float, float2> f;
+    } sh;
+    if (block == 0)
+        tridiag_part_gen<double, double2>(pp.piv, pp.spec, pp.n, pp.nx, (size_t)pp.mp, pp.dy2, M, 0, sh.d);
+    else
+        tridiag_part_gen<float, float2>(pp.pivf, pp.specf, pp.n, pp.nx, (size_t)pp.mp, (float)pp.dy2, M,
+                                        1 + (block - 1) * M, sh.f);
 }
 
 __global__ void __launch_bounds__(TB_THREADS) tridiag_part(const PoissonPlan pp, int M) {
     __shared__ TridiagShared sh;
     tridiag_part_dev(pp, M, blockIdx.x * M, sh);
+}
+
+// Two blocks per SM (64 registers): the FP32 blocks fit; the single FP64
+// zero-mode block spills a little, which costs that one block only.
+__global__ void __launch_bounds__(TB_THREADS, 2) tridiag_part_f32(const PoissonPlan pp, int M) {
+    tridiag_part_f32_dev(pp, M, blockIdx.x);
 }
 
 // ---- batched passes: one launch for many channels -------------------------
@@ -510,6 +666,35 @@ batch_tridiag(const PoissonPlan *__restrict__ plans, const int3 *__restrict__ it
     const int3 it = items[blockIdx.x];
     const PoissonPlan pp = plans[it.x];
     tridiag_part_dev(pp, it.z, it.y, sh);
+}
+
+__global__ void __launch_bounds__(256, 4)
+batch_fwd_rows_f32(const PoissonPlan *__restrict__ plans, const Chan *__restrict__ chans,
+                   double *const *__restrict__ fields, const int2 *__restrict__ items) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ double red[256 / 32];
+    const int2 it = items[blockIdx.x];
+    const PoissonPlan pp = plans[it.x];
+    const Chan &c = chans[it.x];
+    fwd_rows_r16f_dev<256>(pp, fields[it.x] + F_RHS * c.plane, c.nxp, it.y, (float2 *)smraw, red);
+}
+
+__global__ void __launch_bounds__(256, 4)
+batch_inv_rows_f32(const PoissonPlan *__restrict__ plans, const Chan *__restrict__ chans,
+                   double *const *__restrict__ fields, const int2 *__restrict__ items) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int2 it = items[blockIdx.x];
+    const PoissonPlan pp = plans[it.x];
+    const Chan &c = chans[it.x];
+    inv_rows_r16f_dev<256>(pp, c.nxp, c.ny, c.zlo, c.zhi, fields[it.x] + F_PSI * c.plane, it.y, (float2 *)smraw);
+}
+
+// items {channel, block, modes per block}: block 0 is the FP64 zero-mode block
+__global__ void __launch_bounds__(TB_THREADS, 2)
+batch_tridiag_f32(const PoissonPlan *__restrict__ plans, const int3 *__restrict__ items) {
+    const int3 it = items[blockIdx.x];
+    const PoissonPlan pp = plans[it.x];
+    tridiag_part_f32_dev(pp, it.z, it.y);
 }
 
 // Modes per block of tridiag_part for n rows, so that every segment has at
@@ -573,9 +758,44 @@ cudaError_t poisson_pass_f64_at(int pass, const PoissonPlan &pp, const Chan &c, 
 
 int poisson_tridiag_modes(int n) { return tridiag_modes(n); }
 
+bool poisson_f32_supported(const PoissonPlan &pp) {
+    return use_r16(pp) && tridiag_modes(pp.n) > 0 && pp.twf && pp.pivf && pp.specf;
+}
+
+cudaError_t poisson_pass_f32_at(int pass, const PoissonPlan &pp, const Chan &c, const double *rhs, double *psi,
+                                cudaStream_t s) {
+    if (!poisson_f32_supported(pp)) return cudaErrorInvalidValue;
+    if (pass == 1) {
+        const int M = tridiag_modes(pp.n);
+        tridiag_part_f32<<<1 + (pp.nx / 2 + M - 1) / M, TB_THREADS, 0, s>>>(pp, M);
+        return cudaGetLastError();
+    }
+    int threads, per;
+    r16_shape(pp.nx, &threads, &per);
+    const size_t smem = (size_t)per * pp.nx * sizeof(float2);
+    const int blocks = ((pp.n + 1) / 2 + per - 1) / per;
+    if (threads == 256) {
+        if (pass == 0) fwd_rows_r16f<256><<<blocks, 256, smem, s>>>(pp, rhs, c.nxp);
+        else inv_rows_r16f<256><<<blocks, 256, smem, s>>>(pp, c, psi);
+    } else {
+        if (pass == 0) fwd_rows_r16f<512><<<blocks, 512, smem, s>>>(pp, rhs, c.nxp);
+        else inv_rows_r16f<512><<<blocks, 512, smem, s>>>(pp, c, psi);
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t batch_poisson(int pass, const PoissonPlan *plans, const Chan *chans, double *const *fields,
-                          const void *items, int nitems, cudaStream_t s) {
+                          const void *items, int nitems, cudaStream_t s, bool f32) {
     if (nitems <= 0) return cudaSuccess;
+    if (f32) {
+        if (pass == 0)
+            batch_fwd_rows_f32<<<nitems, 256, 32768, s>>>(plans, chans, fields, (const int2 *)items);
+        else if (pass == 1)
+            batch_tridiag_f32<<<nitems, TB_THREADS, 0, s>>>(plans, (const int3 *)items);
+        else
+            batch_inv_rows_f32<<<nitems, 256, 32768, s>>>(plans, chans, fields, (const int2 *)items);
+        return cudaGetLastError();
+    }
     if (pass == 0)
         batch_fwd_rows<<<nitems, 256, 65536, s>>>(plans, chans, fields, (const int2 *)items);
     else if (pass == 1)
@@ -589,7 +809,10 @@ cudaError_t poisson_set_smem_limits() {
     const void *fns[] = {(const void *)fwd_rows, (const void *)inv_rows, (const void *)fwd_rows_r16<256>,
                          (const void *)inv_rows_r16<256>, (const void *)fwd_rows_r16<512>,
                          (const void *)inv_rows_r16<512>, (const void *)batch_fwd_rows,
-                         (const void *)batch_inv_rows};
+                         (const void *)batch_inv_rows, (const void *)fwd_rows_r16f<256>,
+                         (const void *)inv_rows_r16f<256>, (const void *)fwd_rows_r16f<512>,
+                         (const void *)inv_rows_r16f<512>, (const void *)batch_fwd_rows_f32,
+                         (const void *)batch_inv_rows_f32};
     for (const void *f : fns) {
         cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if (e == cudaSuccess)

@@ -118,6 +118,11 @@ class Channel:
         """'auto', 'plain' or 'tma' (shifted storage; both forms are bit-identical)."""
         check(lib().ek_set_option(self._h, 1, {"auto": 0, "plain": 1, "tma": 2}[form]))
 
+    def set_poisson(self, form):
+        """Arithmetic of the Poisson solve: "auto", "f64" or "f32" (row FFTs and
+        column solves of the x-modes >= 1 in FP32, the zero mode in FP64)."""
+        check(lib().ek_set_option(self._h, 2, {"auto": 0, "f64": 1, "f32": 2}[form]))
+
     def rebase(self):
         check(lib().ek_rebase(self._h))
 

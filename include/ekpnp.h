@@ -182,7 +182,14 @@ int ek_set_rebase_interval(ek_ctx *ctx, int32_t steps);
  * (producer warp + mbarrier ring of tensor copies).  Both forms give
  * bit-identical results.  Returns EK_ERR_UNSUPPORTED for a form that this
  * context cannot run. */
-enum { EK_OPT_LBM_KERNEL = 1 };
+enum { EK_OPT_LBM_KERNEL = 1, EK_OPT_POISSON = 2 };
+/* EK_OPT_POISSON selects the arithmetic of the Poisson solve (ek_step and
+ * ek_poisson): 0 = automatic (the FP32 form for FP32/FP16 storage where it
+ * applies, FP64 otherwise), 1 = FP64, 2 = FP32 form: row FFTs and column
+ * solves of the x-modes >= 1 in FP32 on the fluctuation about each row's
+ * mean, the zero mode (row sums, its column solve, the mean of psi) in FP64.
+ * The FP32 form needs shifted storage, a power-of-two nx >= 16 and
+ * ny <= 8194 (EK_ERR_UNSUPPORTED otherwise). */
 int ek_set_option(ek_ctx *ctx, int32_t option, int64_t value);
 
 /* Poisson solve for the current c+, c- moments, then psi and E:

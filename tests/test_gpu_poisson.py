@@ -41,3 +41,49 @@ def test_gpu_poisson_matches_numpy(shape):
     assert rel_err(got["psi"], phi) < tol
     assert np.abs(got["ex"] - ex).max() < tol * np.abs(phi).max()
     assert np.abs(got["ey"] - ey).max() < tol * np.abs(phi).max()
+
+
+F32_SHAPES = [(16, 12), (64, 33), (512, 17), (1024, 129), (4096, 66), (8192, 18), (256, 1500)]
+
+
+@pytest.mark.parametrize("shape", F32_SHAPES, ids=lambda s: f"{s[0]}x{s[1]}")
+@pytest.mark.parametrize("wall", ["uniform", "varying"])
+def test_fp32_poisson_form_against_fp64(shape, wall):
+    """The FP32 form (x-modes >= 1 in FP32 about each row's FP64 mean, zero
+    mode in FP64) against the FP64 solve of the same charges: psi within
+    1e-6 of max |psi|, E within 1e-6 of max |psi| (per lattice spacing)."""
+    import ekpnp
+    nx, ny = shape
+    p = ekpnp.channel_params(nx, ny, kappa_h=5.0, zeta=-1.5, zeta_hi=-0.7, storage=ekpnp.STORE_F32)
+    rng = np.random.default_rng(nx + 3 * ny)
+    x = np.arange(nx)[None, :]
+    y = np.arange(ny)[:, None]
+    smooth = 0.3 * np.sin(np.pi * y / (ny - 1)) * np.cos(2 * np.pi * 3 * x / nx)
+    cp = 1.0 + smooth + 0.1 * rng.standard_normal((ny, nx))
+    cn = 1.0 - smooth + 0.1 * rng.standard_normal((ny, nx))
+    zlo = -2.0 + 1.5 * np.sin(2 * np.pi * np.arange(nx) / max(nx // 4, 1)) if wall == "varying" else None
+    out = {}
+    for form in ("f64", "f32"):
+        with ekpnp.Channel(p) as ch:
+            if zlo is not None:
+                ch.set_wall_profile(zeta_lo=zlo)
+            ch.set_poisson(form)
+            ch.set_fields(cp=cp, cn=cn)
+            ch.poisson()
+            out[form] = ch.get_fields(("psi", "ex", "ey"))
+    ref, got = out["f64"], out["f32"]
+    scale = np.abs(ref["psi"]).max()
+    assert np.abs(got["psi"] - ref["psi"]).max() < 1e-6 * scale
+    assert np.abs(got["ex"] - ref["ex"]).max() < 1e-6 * scale
+    assert np.abs(got["ey"] - ref["ey"]).max() < 1e-6 * scale
+    # the wall rows are the Dirichlet values exactly
+    assert np.array_equal(got["psi"][0], ref["psi"][0]) and np.array_equal(got["psi"][-1], ref["psi"][-1])
+
+
+def test_fp32_poisson_form_is_refused_where_it_does_not_apply():
+    import ekpnp
+    for nx, ny, storage in ((24, 17, ekpnp.STORE_F32), (64, 33, ekpnp.STORE_F64), (8, 30, ekpnp.STORE_F32)):
+        with ekpnp.Channel(ekpnp.channel_params(nx, ny, storage=storage)) as ch:
+            with pytest.raises(ekpnp.EkError):
+                ch.set_poisson("f32")
+            ch.set_poisson("auto")
