@@ -90,6 +90,8 @@ void free_ctx(ek_ctx *c) {
     cudaFree(c->pp.twf);
     cudaFree(c->pp.pivf);
     cudaFree(c->pp.specf);
+    cudaFree(c->pp.rowmean);
+    cudaFree(c->pp.rowmean_ok);
     for (auto &pr : c->ev_pool) {
         cudaEventDestroy(pr.first);
         cudaEventDestroy(pr.second);
@@ -504,6 +506,10 @@ int ek_create(const ek_params *p, ek_ctx **out) {
         if (e == cudaSuccess) e = cudaMalloc(&c->pp.pivf, pivf.size() * sizeof(float));
         if (e == cudaSuccess) e = cudaMalloc(&c->pp.specf, (size_t)c->n * c->mp * sizeof(float2));
         if (e == cudaSuccess) e = cudaMemsetAsync(c->pp.specf, 0, (size_t)c->n * c->mp * sizeof(float2), c->stream);
+        if (e == cudaSuccess) e = cudaMalloc(&c->pp.rowmean, (size_t)c->n * sizeof(double));
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->pp.rowmean, 0, (size_t)c->n * sizeof(double), c->stream);
+        if (e == cudaSuccess) e = cudaMalloc(&c->pp.rowmean_ok, sizeof(int));
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->pp.rowmean_ok, 0, sizeof(int), c->stream);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(c->pp.twf, twf.data(), twf.size() * sizeof(float2), cudaMemcpyHostToDevice, c->stream);
         if (e == cudaSuccess)

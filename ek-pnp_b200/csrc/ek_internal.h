@@ -106,6 +106,8 @@ struct PoissonPlan {
     float2 *twf;                // nx twiddles, FP32
     float *pivf;                // n x mp pivots, FP32
     float2 *specf;              // n x mp spectrum, FP32
+    double *rowmean;            // n row means of the last solve: the offset removed before the FP32 FFT
+    int *rowmean_ok;            // set by the first solve's pass C; before it pass A takes exact means
 };
 // pass 0: row FFTs, 1: tridiagonal column solve, 2: inverse row FFTs + walls
 cudaError_t poisson_pass_f64(int pass, const PoissonPlan &pp, const Chan &c, double *fields, cudaStream_t s);

@@ -411,21 +411,36 @@ __device__ __forceinline__ void fwd_rows_r16f_dev(const PoissonPlan &pp, const d
     const int j0 = 2 * pair, j1 = j0 + 1;
     const bool live = j0 < pp.n, two = j1 < pp.n;
     const double *r0 = rhs + (size_t)(j0 + 1) * nxp, *r1 = rhs + (size_t)(j1 + 1) * nxp;
+    // The FP64 row sums are the zero mode; the FP32 transform takes the
+    // fluctuation about an offset (it only moves the unused FP32 zero bin; a
+    // close one keeps the rounding small).  From the second solve on the
+    // offset is the previous solve's row mean and one pass over the row
+    // does both; the first solve takes two passes and the exact mean.
+    const bool exact = *pp.rowmean_ok == 0;  // the same for every block of the launch
+    double e0 = (live && !exact) ? pp.rowmean[j0] : 0.0, e1 = (two && !exact) ? pp.rowmean[j1] : 0.0;
     double a0 = 0.0, a1 = 0.0;
     for (int x = t; x < N; x += T) {
-        if (live) a0 += __ldg(r0 + x);
-        if (two) a1 += __ldg(r1 + x);
+        const double v0 = live ? __ldg(r0 + x) : 0.0, v1 = two ? __ldg(r1 + x) : 0.0;
+        a0 += v0;
+        a1 += v1;
+        if (!exact) s[swz(x, k)] = make_float2((float)(v0 - e0), (float)(v1 - e1));
     }
     a0 = group_sum<BLOCK>(a0, T, red);
     a1 = group_sum<BLOCK>(a1, T, red);
+    if (exact) {
+        e0 = a0 / (double)N;
+        e1 = a1 / (double)N;
+        for (int x = t; x < N; x += T)
+            s[swz(x, k)] = make_float2(live ? (float)(__ldg(r0 + x) - e0) : 0.0f, two ? (float)(__ldg(r1 + x) - e1) : 0.0f);
+    }
     if (t == 0 && live) {
         pp.spec[(size_t)j0 * pp.mp] = make_double2(a0, 0.0);
-        if (two) pp.spec[(size_t)j1 * pp.mp] = make_double2(a1, 0.0);
+        pp.rowmean[j0] = a0 / (double)N;
+        if (two) {
+            pp.spec[(size_t)j1 * pp.mp] = make_double2(a1, 0.0);
+            pp.rowmean[j1] = a1 / (double)N;
+        }
     }
-    const double m0 = a0 / (double)N, m1 = a1 / (double)N;
-    for (int x = t; x < N; x += T)
-        s[swz(x, k)] = live ? make_float2((float)(__ldg(r0 + x) - m0), two ? (float)(__ldg(r1 + x) - m1) : 0.0f)
-                            : make_float2(0.0f, 0.0f);
     __syncthreads();
     reg_fft<false, float2>(s, k, T, t, pp.twf);
     if (!live) return;
@@ -458,6 +473,7 @@ __device__ __forceinline__ void inv_rows_r16f_dev(const PoissonPlan &pp, int nxp
     __syncthreads();
     reg_fft<true, float2>(s, k, T, t, pp.twf);
     const double inv = 1.0 / (double)N;
+    if (pair_base == 0 && threadIdx.x == 0) *pp.rowmean_ok = 1;
     if (live) {
         const double mean0 = pp.spec[(size_t)j0 * pp.mp].x * inv;
         const double mean1 = two ? pp.spec[(size_t)j1 * pp.mp].x * inv : 0.0;
@@ -759,7 +775,7 @@ cudaError_t poisson_pass_f64_at(int pass, const PoissonPlan &pp, const Chan &c, 
 int poisson_tridiag_modes(int n) { return tridiag_modes(n); }
 
 bool poisson_f32_supported(const PoissonPlan &pp) {
-    return use_r16(pp) && tridiag_modes(pp.n) > 0 && pp.twf && pp.pivf && pp.specf;
+    return use_r16(pp) && tridiag_modes(pp.n) > 0 && pp.twf && pp.pivf && pp.specf && pp.rowmean && pp.rowmean_ok;
 }
 
 cudaError_t poisson_pass_f32_at(int pass, const PoissonPlan &pp, const Chan &c, const double *rhs, double *psi,
