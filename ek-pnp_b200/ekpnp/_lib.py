@@ -106,6 +106,16 @@ _SIGS = {
     "ek_batch_residual": ([ctypes.c_void_p, ctypes.c_int32, _dp, _dp], ctypes.c_int),
     "ek_batch_set_active": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "ek_batch_active": ([ctypes.c_void_p, ctypes.c_void_p, _P(ctypes.c_int64)], ctypes.c_int),
+    "ek_write_restart": ([ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_double] + [_dp] * 8, ctypes.c_int),
+    "ek_read_restart": ([ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, _dp] + [_dp] * 8, ctypes.c_int),
+    "ek_save_restart": ([ctypes.c_void_p, ctypes.c_char_p, ctypes.c_double], ctypes.c_int),
+    "ek_load_restart": ([ctypes.c_void_p, ctypes.c_char_p, _dp], ctypes.c_int),
+    "ek_write_tecplot": ([ctypes.c_char_p, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, ctypes.c_int32,
+                          ctypes.c_double, ctypes.c_double] + [_dp] * 8, ctypes.c_int),
+    "ek_write_dmd": ([ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _dp], ctypes.c_int),
+    "ek_diag_current": ([ctypes.c_int32, ctypes.c_int32, _dp, _dp, ctypes.c_double, ctypes.c_double, _dp],
+                        ctypes.c_int),
+    "ek_diag_umax": ([ctypes.c_int32, ctypes.c_int32, _dp, _dp], ctypes.c_int),
     "ek_mlp_create": ([ctypes.c_int32, ctypes.c_uint64, _P(ctypes.c_void_p)], ctypes.c_int),
     "ek_mlp_destroy": ([ctypes.c_void_p], ctypes.c_int),
     "ek_mlp_param_count": ([ctypes.c_void_p, _P(ctypes.c_int64)], ctypes.c_int),

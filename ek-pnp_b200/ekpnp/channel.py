@@ -118,6 +118,18 @@ class Channel:
         """'auto', 'plain' or 'tma' (shifted storage; both forms are bit-identical)."""
         check(lib().ek_set_option(self._h, 1, {"auto": 0, "plain": 1, "tma": 2}[form]))
 
+    def save_restart(self, path, time=0.0):
+        """The channel's fields as the reference's data_end.dat (save_data_end)."""
+        import os
+        check(lib().ek_save_restart(self._h, os.fsencode(path), float(time)))
+
+    def load_restart(self, path):
+        """Fields from a data_end.dat file (read_data); returns its time."""
+        import os
+        t = ctypes.c_double(0.0)
+        check(lib().ek_load_restart(self._h, os.fsencode(path), ctypes.byref(t)))
+        return float(t.value)
+
     def set_poisson(self, form):
         """Arithmetic of the Poisson solve: "auto", "f64" or "f32" (row FFTs and
         column solves of the x-modes >= 1 in FP32, the zero mode in FP64)."""

@@ -261,6 +261,38 @@ int ek_elapsed(ek_ctx *ctx, int32_t slot_a, int32_t slot_b, double *ms);
 /* Total number of kernels this context has launched. */
 int ek_launch_count(const ek_ctx *ctx, int64_t *out);
 
+/* ---- the reference's file formats and diagnostics (host arrays) ---------
+ * Field arrays are nx*ny doubles, index nx*y + x; no device work.  The
+ * reference extrapolates wall rows of its own host copies in place; these
+ * calls leave the caller's arrays unchanged. */
+/* data_end.dat restart: nx*ny lines "%10.6f" x 9: time ux uy rho c+ phi Ex Ey
+ * c- (save_data_end LBM.cu:1272-1312; read_data LBM.cu:1350-1392). */
+int ek_write_restart(const char *path, int32_t nx, int32_t ny, double time, const double *ux, const double *uy,
+                     const double *rho, const double *cp, const double *psi, const double *ex, const double *ey,
+                     const double *cn);
+int ek_read_restart(const char *path, int32_t nx, int32_t ny, double *time, double *ux, double *uy, double *rho,
+                    double *cp, double *psi, double *ex, double *ey, double *cn);
+/* A context's fields to / from that file (ek_load_restart also loads E,
+ * which the next step then uses, as read_data's Ex/Ey are). */
+int ek_save_restart(ek_ctx *ctx, const char *path, double time);
+int ek_load_restart(ek_ctx *ctx, const char *path, double *time);
+/* One Tecplot POINT zone with the reference's derived fields (charge
+ * gradient, vorticity and its Laplacian, curl of the electric force); the
+ * VARIABLES header and a new file when first != 0, appended otherwise
+ * (save_data_tecplot LBM.cu:1100-1270).  nx >= 3, ny >= 6. */
+int ek_write_tecplot(const char *path, int32_t first, double time, int32_t nx, int32_t ny, double dx, double dy,
+                     const double *ux, const double *uy, const double *rho, const double *cp, const double *psi,
+                     const double *ex, const double *ey, const double *cn);
+/* c+ snapshot for DMD, top row extrapolated, "%10.6f \n" per node
+ * (save_data_dmd LBM.cu:1314-1348). */
+int ek_write_dmd(const char *path, int32_t append, int32_t nx, int32_t ny, const double *cp);
+/* Electric current through the top wall, K dy sum_x c+ Ey on the
+ * extrapolated wall row (current LBM.cu:1394-1417); mob_p is K. */
+int ek_diag_current(int32_t nx, int32_t ny, const double *cp, const double *ey, double mob_p, double dy, double *out);
+/* The reference's "umax": the maximum of u_y (not |u|) with the top row
+ * extrapolated, never below 0 (record_umax LBM.cu:1419-1451). */
+int ek_diag_umax(int32_t nx, int32_t ny, const double *uy, double *out);
+
 /* ---- batches of independent channels ------------------------------------
  * No counterpart in the reference (one channel per run of main.cu).  A batch
  * steps many channels of different sizes and parameters in lockstep, four
