@@ -50,6 +50,12 @@ ChanF make_chanf(const Chan &c) {
     k.exf = c.exf;
     k.dx = c.dx;
     k.dy = c.dy;
+    k.wcpd = c.r.wcp;
+    k.wcmd = c.r.wcm;
+    k.wtpd = c.r.wtp;
+    k.wtmd = c.r.wtm;
+    k.mob_pd = c.mob_p;
+    k.mob_nd = c.mob_n;
     k.half_inv_dx = 0.5 / c.dx;
     k.half_inv_dy = 0.5 / c.dy;
     k.rhs_q = -c.f_charge / c.eps;
