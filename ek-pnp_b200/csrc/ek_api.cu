@@ -1,7 +1,8 @@
 // ek_api.cu -- the C ABI of libekpnp (declared in include/ekpnp.h).
 //
 // Host-side owner of a channel: allocation, parameter checks, the step loop
-// (one fused LBM launch + three Poisson launches per step) and field I/O.
+// (one fused LBM launch + three Poisson passes per step, the column pass of
+// the FP32 Poisson form as two kernels on two streams) and field I/O.
 // Replaces the host code of main.cu:28-307 and the host wrappers of LBM.cu /
 // poisson.cu; every failure is returned as a status instead of exit().
 #include <cuda.h>
@@ -98,6 +99,9 @@ void free_ctx(ek_ctx *c) {
     }
     for (auto &m : c->marks)
         if (m) cudaEventDestroy(m);
+    if (c->fork) cudaEventDestroy(c->fork);
+    if (c->join) cudaEventDestroy(c->join);
+    if (c->side) cudaStreamDestroy(c->side);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -237,7 +241,7 @@ int refresh_e(ek_ctx *c) {
 // Launch one kernel of `phase` through fn(); with profiling on, bracket it
 // with a pair of events from the context's pool.
 template <typename Fn>
-int timed(ek_ctx *c, int phase, const char *what, Fn fn) {
+int timed(ek_ctx *c, int phase, const char *what, Fn fn, int kernels = 1) {
     cudaEvent_t a = nullptr, b = nullptr;
     if (c->prof) {
         if (c->ev_used == c->ev_pool.size()) {
@@ -254,19 +258,39 @@ int timed(ek_ctx *c, int phase, const char *what, Fn fn) {
         EK_CUDA(cudaEventRecord(a, c->stream), "event record");
     }
     EK_CUDA(fn(), what);
-    ++c->launches;
+    c->launches += kernels;
     if (c->prof) EK_CUDA(cudaEventRecord(b, c->stream), "event record");
     return EK_OK;
 }
 
+// Side stream and fork/join events of the split column solve, made on first use.
+int side_stream(ek_ctx *c) {
+    if (c->side) return EK_OK;
+    EK_CUDA(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming), "event create");
+    EK_CUDA(cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming), "event create");
+    EK_CUDA(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking), "stream create");
+    return EK_OK;
+}
+
 int poisson_now(ek_ctx *c) {
+    const bool f32 = ek::ctx_poisson_f32(c);
+    if (f32) {
+        int rc = side_stream(c);
+        if (rc != EK_OK) return rc;
+    }
     for (int pass = 0; pass < 3; ++pass) {
-        const bool f32 = ek::ctx_poisson_f32(c);
-        int rc = timed(c, 1 + pass, "poisson kernel", [&] {
-            return f32 ? poisson_pass_f32_at(pass, c->pp, c->chan, c->fields + F_RHS * c->plane,
-                                             c->fields + F_PSI * c->plane, c->stream)
-                       : poisson_pass_f64(pass, c->pp, c->chan, c->fields, c->stream);
-        });
+        // FP32 form, pass B: FP64 zero mode on the side stream beside the
+        // FP32 modes (two kernels)
+        const bool split = f32 && pass == 1;
+        int rc = timed(
+            c, 1 + pass, "poisson kernel",
+            [&] {
+                if (split) return poisson_tridiag_f32_split(c->pp, c->stream, c->side, c->fork, c->join);
+                return f32 ? poisson_pass_f32_at(pass, c->pp, c->chan, c->fields + F_RHS * c->plane,
+                                                 c->fields + F_PSI * c->plane, c->stream)
+                           : poisson_pass_f64(pass, c->pp, c->chan, c->fields, c->stream);
+            },
+            split ? 2 : 1);
         if (rc != EK_OK) return rc;
     }
     if (c->p.flags & EK_FLAG_EXPLICIT_E) {

@@ -3,7 +3,8 @@
 //
 // Each channel keeps its own context (ek_ctx: populations, fields, Poisson
 // plan, wall profiles, reference rows) and all of them step in lockstep with
-// four launches per step, whatever the number of channels:
+// four launches per step (five with the FP32 Poisson form, whose column solve
+// runs the FP64 zero modes on a side stream), whatever the number of channels:
 //   LBM      one persistent kernel over a host-built tile work-list.  A tile is
 //            {channel, first row, first column, width}; channels narrower
 //            than the block put several rows into one tile.  Every block walks
@@ -169,6 +170,8 @@ struct ek_batch {
     std::vector<int64_t> ch_steps;   // steps each channel has taken in the batch
     int storage = EK_STORE_F32;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;     // FP32 Poisson form: the FP64 zero modes run here
+    cudaEvent_t fork = nullptr, join = nullptr;
     int cur = 0;                     // population buffer holding the current state (all channels)
     bool state_pre = false;
     bool explicit_e_once = false;
@@ -195,6 +198,8 @@ struct ek_batch {
     int npairs = 0;
     int3 *d_modes = nullptr;         // Poisson x-mode items
     int nmodes = 0;
+    int3 *d_zeros = nullptr;         // FP32 form: the FP64 zero-mode items
+    int nzeros = 0;
     int2 *d_rows = nullptr;          // {channel, row} of every row
     int nrows = 0;
     // residuals
@@ -229,6 +234,9 @@ int upload(T **dst, const std::vector<T> &v, cudaStream_t s) {
     EK_BCUDA(cudaStreamSynchronize(s), "batch table");
     return EK_OK;
 }
+
+// LBM + three Poisson passes; the FP32 form's column solve is two kernels.
+int launches_per_step(const ek_batch *b) { return b->poisson_f32 ? 5 : 4; }
 
 void release_graph(ek_batch *b) {
     if (b->graph) cudaGraphExecDestroy(b->graph);
@@ -270,7 +278,7 @@ int build_tables(ek_batch *b) {
     std::vector<float *> sp;
     std::vector<int4> kq, ritems;
     std::vector<int2> pairs, rows, rranges;
-    std::vector<int3> modes;
+    std::vector<int3> modes, zeros;
     release_graph(b);
     b->kcur.clear();
     int nrpart = 0;
@@ -297,8 +305,9 @@ int build_tables(ek_batch *b) {
             const int per = 256 / (nx >> 4);
             for (int q = 0; q < (n + 1) / 2; q += per) pairs.push_back(make_int2((int)i, q));
             const int M = poisson_tridiag_modes(n);
-            if (f32) {  // block 0: the FP64 zero mode; blocks 1..: modes 1.. in FP32
-                for (int blk = 0; blk <= (nx / 2 + M - 1) / M; ++blk) modes.push_back(make_int3((int)i, blk, M));
+            if (f32) {  // the zero mode in FP64 (modes 0..M-1 of the FP64 spectrum); modes 1.. in FP32
+                zeros.push_back(make_int3((int)i, 0, M));
+                for (int m0 = 1; m0 <= nx / 2; m0 += M) modes.push_back(make_int3((int)i, m0, M));
             } else {
                 for (int m0 = 0; m0 <= nx / 2; m0 += M) modes.push_back(make_int3((int)i, m0, M));
             }
@@ -321,11 +330,13 @@ int build_tables(ek_batch *b) {
     if ((rc = upload(&b->d_kq, kq, b->stream)) != EK_OK) return rc;
     if ((rc = upload(&b->d_pairs, pairs, b->stream)) != EK_OK) return rc;
     if ((rc = upload(&b->d_modes, modes, b->stream)) != EK_OK) return rc;
+    if ((rc = upload(&b->d_zeros, zeros, b->stream)) != EK_OK) return rc;
     if ((rc = upload(&b->d_rows, rows, b->stream)) != EK_OK) return rc;
     if ((rc = upload(&b->d_ritems, ritems, b->stream)) != EK_OK) return rc;
     if ((rc = upload(&b->d_rranges, rranges, b->stream)) != EK_OK) return rc;
     b->npairs = (int)pairs.size();
     b->nmodes = (int)modes.size();
+    b->nzeros = (int)zeros.size();
     b->nrows = (int)rows.size();
     b->nritems = (int)ritems.size();
     if (b->d_rpart) cudaFree(b->d_rpart);
@@ -346,9 +357,15 @@ int launch_step(ek_batch *b, bool first, bool ee, bool mom) {
                                        first, ee, mom, b->stream);
     EK_BCUDA(e, "batch LBM kernel");
     EK_BCUDA(batch_poisson(0, b->d_plans, b->d_chan, b->d_fields, b->d_pairs, b->npairs, b->stream, b->poisson_f32), "batch rows");
-    EK_BCUDA(batch_poisson(1, b->d_plans, b->d_chan, b->d_fields, b->d_modes, b->nmodes, b->stream, b->poisson_f32), "batch modes");
+    if (b->poisson_f32)
+        EK_BCUDA(batch_tridiag_f32_split(b->d_plans, b->d_zeros, b->nzeros, b->d_modes, b->nmodes, b->stream,
+                                         b->side, b->fork, b->join),
+                 "batch modes");
+    else
+        EK_BCUDA(batch_poisson(1, b->d_plans, b->d_chan, b->d_fields, b->d_modes, b->nmodes, b->stream, false),
+                 "batch modes");
     EK_BCUDA(batch_poisson(2, b->d_plans, b->d_chan, b->d_fields, b->d_pairs, b->npairs, b->stream, b->poisson_f32), "batch rows");
-    b->launches += 4;
+    b->launches += launches_per_step(b);
     b->cur ^= 1;
     return EK_OK;
 }
@@ -425,7 +442,7 @@ int check_channels(ek_batch *b) {
     return EK_OK;
 }
 
-int launches_per_cycle(const ek_batch *b) { return b->cycle * 4 + (b->rebase ? 3 : 0); }
+int launches_per_cycle(const ek_batch *b) { return b->cycle * launches_per_step(b) + (b->rebase ? 3 : 0); }
 
 }  // namespace
 
@@ -451,6 +468,13 @@ int ek_batch_create(const ek_params *params, int32_t count, ek_batch **out) {
     cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         b->stream = nullptr;
+        ek_batch_destroy(b);
+        return cuda_err(e, "stream create");
+    }
+    e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
         ek_batch_destroy(b);
         return cuda_err(e, "stream create");
     }
@@ -485,9 +509,12 @@ int ek_batch_destroy(ek_batch *b) {
     for (ek_ctx *c : b->ch) ek_destroy(c);  // the channels do not own the batch's stream
     void *tables[] = {b->d_chanf, b->d_chan,  b->d_plans,  b->d_pops[0],  b->d_pops[1], b->d_fields,
                       b->d_spare, b->d_kq,    b->d_tiles,  b->d_pairs,    b->d_modes,   b->d_rows,
-                      b->d_snaps, b->d_ritems, b->d_rranges, b->d_rpart};
+                      b->d_snaps, b->d_ritems, b->d_rranges, b->d_rpart,  b->d_zeros};
     for (void *t : tables)
         if (t) cudaFree(t);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->join) cudaEventDestroy(b->join);
+    if (b->side) cudaStreamDestroy(b->side);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return EK_OK;

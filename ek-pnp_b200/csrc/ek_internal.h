@@ -122,6 +122,12 @@ size_t poisson_smem_bytes_f64(int nx);
 bool poisson_f32_supported(const PoissonPlan &pp);
 cudaError_t poisson_pass_f32_at(int pass, const PoissonPlan &pp, const Chan &c, const double *rhs, double *psi,
                                 cudaStream_t s);
+// Pass B of the FP32 form as two kernels on two streams: the FP64 zero mode
+// on `side`, the FP32 modes on `s` (fork/join through the two events).
+cudaError_t poisson_tridiag_f32_split(const PoissonPlan &pp, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
+                                      cudaEvent_t join);
+cudaError_t batch_tridiag_f32_split(const PoissonPlan *plans, const void *zero_items, int nzero, const void *mode_items,
+                                    int nmodes, cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join);
 // Batched Poisson passes over many channels (ek_batch.cu builds the items):
 // pass 0/2 items int2 {channel, first row pair} (256-thread blocks, each
 // 256/(nx/16) row pairs; power-of-two nx from 16 to 4096); pass 1 items

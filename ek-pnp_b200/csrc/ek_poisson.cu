@@ -664,6 +664,20 @@ __global__ void __launch_bounds__(TB_THREADS, 2) tridiag_part_f32(const PoissonP
     tridiag_part_f32_dev(pp, M, blockIdx.x);
 }
 
+// Split form of the FP32 pass B: the FP64 zero-mode block on its own (no
+// register cap, so no spills), the FP32 mode blocks with two blocks per SM;
+// the caller runs the two on two streams.
+__global__ void __launch_bounds__(TB_THREADS) tridiag_zero_f64(const PoissonPlan pp, int M) {
+    __shared__ TridiagShared sh;
+    tridiag_part_dev(pp, M, 0, sh);
+}
+
+__global__ void __launch_bounds__(TB_THREADS, 2) tridiag_modes_f32(const PoissonPlan pp, int M) {
+    __shared__ TridiagSharedT<float, float2> sh;
+    tridiag_part_gen<float, float2>(pp.pivf, pp.specf, pp.n, pp.nx, (size_t)pp.mp, (float)pp.dy2, M,
+                                    1 + blockIdx.x * M, sh);
+}
+
 // ---- batched passes: one launch for many channels -------------------------
 // A block's work item names its channel and its first row pair (passes A,
 // C) or first x-mode (pass B); the channel's plan comes from a device table.
@@ -714,6 +728,16 @@ batch_inv_rows_f32(const PoissonPlan *__restrict__ plans, const Chan *__restrict
     const PoissonPlan pp = plans[it.x];
     const Chan &c = chans[it.x];
     inv_rows_r16f_dev<256>(pp, c.nxp, c.ny, c.zlo, c.zhi, fields[it.x] + F_PSI * c.plane, it.y, (float2 *)smraw);
+}
+
+// items {channel, first mode, modes per block}: FP32 mode blocks (the zero
+// mode runs in batch_tridiag, FP64)
+__global__ void __launch_bounds__(TB_THREADS, 2)
+batch_tridiag_modes_f32(const PoissonPlan *__restrict__ plans, const int3 *__restrict__ items) {
+    __shared__ TridiagSharedT<float, float2> sh;
+    const int3 it = items[blockIdx.x];
+    const PoissonPlan pp = plans[it.x];
+    tridiag_part_gen<float, float2>(pp.pivf, pp.specf, pp.n, pp.nx, (size_t)pp.mp, (float)pp.dy2, it.z, it.y, sh);
 }
 
 // items {channel, block, modes per block}: block 0 is the FP64 zero-mode block
@@ -789,6 +813,21 @@ bool poisson_f32_supported(const PoissonPlan &pp) {
     return use_r16(pp) && tridiag_modes(pp.n) > 0 && pp.twf && pp.pivf && pp.specf && pp.rowmean && pp.rowmean_ok;
 }
 
+cudaError_t poisson_tridiag_f32_split(const PoissonPlan &pp, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
+                                      cudaEvent_t join) {
+    if (!poisson_f32_supported(pp)) return cudaErrorInvalidValue;
+    const int M = tridiag_modes(pp.n);
+    cudaError_t e = cudaEventRecord(fork, s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(side, fork, 0);
+    if (e != cudaSuccess) return e;
+    tridiag_zero_f64<<<1, TB_THREADS, 0, side>>>(pp, M);
+    tridiag_modes_f32<<<(pp.nx / 2 + M - 1) / M, TB_THREADS, 0, s>>>(pp, M);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaEventRecord(join, side);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, join, 0);
+    return e;
+}
+
 cudaError_t poisson_pass_f32_at(int pass, const PoissonPlan &pp, const Chan &c, const double *rhs, double *psi,
                                 cudaStream_t s) {
     if (!poisson_f32_supported(pp)) return cudaErrorInvalidValue;
@@ -830,6 +869,19 @@ cudaError_t batch_poisson(int pass, const PoissonPlan *plans, const Chan *chans,
     else
         batch_inv_rows<<<nitems, 256, 65536, s>>>(plans, chans, fields, (const int2 *)items);
     return cudaGetLastError();
+}
+
+cudaError_t batch_tridiag_f32_split(const PoissonPlan *plans, const void *zero_items, int nzero, const void *mode_items,
+                                    int nmodes, cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join) {
+    cudaError_t e = cudaEventRecord(fork, s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(side, fork, 0);
+    if (e != cudaSuccess) return e;
+    if (nzero > 0) batch_tridiag<<<nzero, TB_THREADS, 0, side>>>(plans, (const int3 *)zero_items);
+    if (nmodes > 0) batch_tridiag_modes_f32<<<nmodes, TB_THREADS, 0, s>>>(plans, (const int3 *)mode_items);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaEventRecord(join, side);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, join, 0);
+    return e;
 }
 
 cudaError_t poisson_set_smem_limits() {

@@ -2,7 +2,7 @@
 
 The reference runs one channel per process (main.cu); a Batch runs hundreds
 of channels of different sizes and parameters with four kernel launches per
-step for all of them.  Each channel is a Channel view (fields in and out,
+step for all of them (five with the FP32 Poisson form).  Each channel is a Channel view (fields in and out,
 wall profiles, Poisson-Boltzmann start, residual) that is stepped only
 through the batch.
 """

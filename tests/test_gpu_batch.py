@@ -136,8 +136,9 @@ def test_launch_count_is_independent_of_channel_count():
             b.step(40)
             b.sync()
             counts.append(b.launches - before)
-    # 4 launches per step + 3 re-basing launches per cycle, whatever the batch size
-    assert counts[0] == counts[1] == 40 * 4 + 4 * 3
+    # 5 launches per step (FP32 Poisson form: two column-solve kernels) + 3
+    # re-basing launches per cycle, whatever the batch size
+    assert counts[0] == counts[1] == 40 * 5 + 4 * 3
 
 
 def test_stepping_a_channel_alone_is_refused():
