@@ -522,10 +522,18 @@ int ek_create(const ek_params *p, ek_ctx **out) {
     c->pp.log2nx = c->pp.pow2 ? lg : 0;
     c->pp.dy2 = p->dy * p->dy;
     if (p->storage != EK_STORE_F64 && c->pp.pow2 && p->nx >= 16 && poisson_tridiag_modes(c->n) > 0) {
-        // FP32 form of the Poisson solve: FP32 twiddles, pivots and spectrum
+        // FP32 form of the Poisson solve: FP32 pivots and spectrum; the row
+        // transforms' twiddles per radix-16 pass on bits [b, b+4), b = lg-4,
+        // lg-8, ... >= 1: exp(-2 pi i kb f / 2^(b+4)) at (f-1) 2^b + kb
         std::vector<float> pivf(piv.begin(), piv.end());
-        std::vector<float2> twf(tw.size());
-        for (size_t i = 0; i < tw.size(); ++i) twf[i] = make_float2((float)tw[i].x, (float)tw[i].y);
+        std::vector<float2> twf;
+        for (int b = lg - 4; b >= 1; b -= 4)
+            for (int f = 1; f < 16; ++f)
+                for (int kb = 0; kb < (1 << b); ++kb) {
+                    const double2 w = tw[((size_t)kb * f << (lg - b - 4)) % (size_t)p->nx];
+                    twf.push_back(make_float2((float)w.x, (float)w.y));
+                }
+        if (twf.empty()) twf.push_back(make_float2(1.0f, 0.0f));
         e = cudaMalloc(&c->pp.twf, twf.size() * sizeof(float2));
         if (e == cudaSuccess) e = cudaMalloc(&c->pp.pivf, pivf.size() * sizeof(float));
         if (e == cudaSuccess) e = cudaMalloc(&c->pp.specf, (size_t)c->n * c->mp * sizeof(float2));

@@ -103,7 +103,7 @@ struct PoissonPlan {
     double2 *spec;              // n x mp spectrum
     // FP32 form (shifted storage): modes >= 1 in FP32, the zero mode in FP64
     // (column 0 of spec); null where the form is not set up
-    float2 *twf;                // nx twiddles, FP32
+    float2 *twf;                // FP32 row transforms: per-pass twiddle tables (< nx entries)
     float *pivf;                // n x mp pivots, FP32
     float2 *specf;              // n x mp spectrum, FP32
     double *rowmean;            // n row means of the last solve: the offset removed before the FP32 FFT

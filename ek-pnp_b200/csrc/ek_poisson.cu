@@ -20,6 +20,7 @@
 // The result equals the reference's to rounding (the test suite compares).
 #include <cuda_runtime.h>
 
+#include "ek_fft32.cuh"
 #include "ek_internal.h"
 
 namespace ek {
@@ -33,11 +34,6 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
-__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
 template <typename C> __device__ __forceinline__ C cmake(double a, double b);
 template <> __device__ __forceinline__ double2 cmake<double2>(double a, double b) { return make_double2(a, b); }
@@ -136,11 +132,27 @@ __global__ void __launch_bounds__(PTPB) tridiag(const PoissonPlan pp) {
     }
 }
 
-// Pass C: spectra of rows (y0, y1) -> psi rows; block 0 also writes the walls.
+// Wall rows psi[0] = zlo, psi[ny-1] = zhi (odd_extract, poisson.cu:297-304),
+// spread over the nb blocks of one channel's inverse pass (lb = this block's
+// index among them, bs threads a block) and issued at the start of the
+// pass: one block writing both rows alone made a chain of dependent loads
+// that outlasted the rest of the pass.
+__device__ __forceinline__ void write_walls(double *__restrict__ psi, const double *__restrict__ zlo,
+                                            const double *__restrict__ zhi, int nx, int ny, int nxp, int lb,
+                                            int nb, int bs) {
+    double *lo = psi, *hi = psi + (size_t)(ny - 1) * nxp;
+    for (int g = lb * bs + (int)threadIdx.x; g < 2 * nx; g += nb * bs) {
+        if (g < nx) lo[g] = __ldg(zlo + g);
+        else hi[g - nx] = __ldg(zhi + g - nx);
+    }
+}
+
+// Pass C: spectra of rows (y0, y1) -> psi rows; the walls spread over the blocks.
 __global__ void __launch_bounds__(PTPB)
 inv_rows(const PoissonPlan pp, const Chan c, double *__restrict__ psi) {
     extern __shared__ double2 sm[];
     const int nx = pp.nx, nxp = c.nxp;
+    write_walls(psi, c.zlo, c.zhi, nx, c.ny, nxp, blockIdx.x, gridDim.x, blockDim.x);
     const int j0 = 2 * blockIdx.x, j1 = j0 + 1;
     const bool two = j1 < pp.n;
     const double2 *s0 = pp.spec + (size_t)j0 * pp.mp, *s1 = pp.spec + (size_t)j1 * pp.mp;
@@ -170,14 +182,6 @@ inv_rows(const PoissonPlan pp, const Chan c, double *__restrict__ psi) {
         p0[x] = z[x].x * inv;
         if (two) p1[x] = z[x].y * inv;
     }
-    if (blockIdx.x == 0) {
-        // wall rows hold the wall potential (odd_extract, poisson.cu:297-304)
-        double *lo = psi, *hi = psi + (size_t)(c.ny - 1) * nxp;
-        for (int x = threadIdx.x; x < nx; x += blockDim.x) {
-            lo[x] = c.zlo[x];
-            hi[x] = c.zhi[x];
-        }
-    }
 }
 
 // ---- register-blocked radix-16 row FFTs (power-of-two nx >= 16) ----------
@@ -205,16 +209,10 @@ __device__ __forceinline__ int swz(int i, int k) {
     return i ^ (((i >> 4) ^ rtop) & 7);
 }
 
-// Shared-memory index of element i of transform p in a block: the FP64 form
-// uses swz (16-byte elements); the FP32 form (8-byte elements) XORs the low
-// four index bits with bits 4-7, 8-11 and the transform number, which keeps
-// the register passes, the natural-order and the bit-reversed accesses free
-// of bank conflicts for 256 <= nx <= 4096 at a third of swz's cost.
+// Shared-memory index of element i of a transform (the FP64 form; the FP32
+// row transforms of ek_fft32.cuh have their own map).
 template <typename C> __device__ __forceinline__ int sidx(int i, int k, int p);
 template <> __device__ __forceinline__ int sidx<double2>(int i, int k, int) { return swz(i, k); }
-template <> __device__ __forceinline__ int sidx<float2>(int i, int, int p) {
-    return i ^ (((i >> 4) ^ (i >> 8) ^ p) & 15);
-}
 
 // exp(-2 pi i v/2^(sl+1)) for 0 <= v < 2^sl <= 8 (compile-time arguments)
 template <typename C>
@@ -341,8 +339,7 @@ fwd_rows_r16(const PoissonPlan pp, const double *__restrict__ rhs, int nxp) {
     fwd_rows_r16_dev<BLOCK>(pp, rhs, nxp, blockIdx.x * (BLOCK / (pp.nx >> 4)), sm);
 }
 
-// Pass C, radix-16 form: spectra -> psi rows; the block holding row pair 0
-// also writes the walls.
+// Pass C, radix-16 form: spectra -> psi rows and the walls.
 template <int BLOCK>
 __device__ __forceinline__ void inv_rows_r16_dev(const PoissonPlan &pp, int nxp, int ny, const double *zlo,
                                                  const double *zhi, double *__restrict__ psi, int pair_base,
@@ -353,6 +350,8 @@ __device__ __forceinline__ void inv_rows_r16_dev(const PoissonPlan &pp, int nxp,
     double2 *s = sm + p * N;
     const int j0 = 2 * pair, j1 = j0 + 1;
     const bool live = j0 < pp.n, two = j1 < pp.n;
+    const int per = BLOCK / T;
+    write_walls(psi, zlo, zhi, N, ny, nxp, pair_base / per, ((pp.n + 1) / 2 + per - 1) / per, BLOCK);
     const double2 *s0 = pp.spec + (size_t)j0 * pp.mp, *s1 = pp.spec + (size_t)j1 * pp.mp;
     for (int m = t; m <= N / 2; m += T) {
         const double2 a = live ? s0[m] : make_double2(0.0, 0.0);
@@ -369,13 +368,6 @@ __device__ __forceinline__ void inv_rows_r16_dev(const PoissonPlan &pp, int nxp,
             const double2 z = s[swz(x, k)];
             p0[x] = z.x * inv;
             if (two) p1[x] = z.y * inv;
-        }
-    }
-    if (pair_base == 0) {
-        double *lo = psi, *hi = psi + (size_t)(ny - 1) * nxp;
-        for (int x = threadIdx.x; x < N; x += BLOCK) {
-            lo[x] = zlo[x];
-            hi[x] = zhi[x];
         }
     }
 }
@@ -412,37 +404,43 @@ __device__ __forceinline__ double group_sum(double v, int T, double *red) {
     return s;
 }
 
-template <int BLOCK>
-__device__ __forceinline__ void fwd_rows_r16f_dev(const PoissonPlan &pp, const double *__restrict__ rhs, int nxp,
-                                                  int pair_base, float2 *sm, double *red) {
-    const int N = pp.nx, k = pp.log2nx, T = N >> 4;
+// Pass A of the FP32 form for 2^K-point rows: the FP64 row sums (the zero
+// mode) and the FP32 transform of the fluctuation about an offset (it only
+// moves the unused FP32 zero bin; a close one keeps the rounding small).
+// From the second solve on the offset is the previous solve's row mean and
+// one pass over the row does both; the first solve takes two passes and the
+// exact mean.  The first radix-16 pass runs on the values as loaded.
+template <int BLOCK, int K>
+__device__ __forceinline__ void fwd_rows_f32_k(const PoissonPlan &pp, const double *__restrict__ rhs, int nxp,
+                                               int pair_base, float2 *sm, double *red) {
+    using S = fft32::Shape<K>;
+    constexpr int N = S::N, T = S::T;
     const int p = threadIdx.x / T, t = threadIdx.x - p * T;
     const int pair = pair_base + p;
     float2 *s = sm + p * N;
     const int j0 = 2 * pair, j1 = j0 + 1;
     const bool live = j0 < pp.n, two = j1 < pp.n;
-    const double *r0 = rhs + (size_t)(j0 + 1) * nxp, *r1 = rhs + (size_t)(j1 + 1) * nxp;
-    // The FP64 row sums are the zero mode; the FP32 transform takes the
-    // fluctuation about an offset (it only moves the unused FP32 zero bin; a
-    // close one keeps the rounding small).  From the second solve on the
-    // offset is the previous solve's row mean and one pass over the row
-    // does both; the first solve takes two passes and the exact mean.
+    const double *r0 = rhs + (size_t)(j0 + 1) * nxp + t, *r1 = rhs + (size_t)(j1 + 1) * nxp + t;
     const bool exact = *pp.rowmean_ok == 0;  // the same for every block of the launch
     double e0 = (live && !exact) ? pp.rowmean[j0] : 0.0, e1 = (two && !exact) ? pp.rowmean[j1] : 0.0;
     double a0 = 0.0, a1 = 0.0;
-    for (int x = t; x < N; x += T) {
-        const double v0 = live ? __ldg(r0 + x) : 0.0, v1 = two ? __ldg(r1 + x) : 0.0;
+    float2 x[16];
+#pragma unroll
+    for (int v = 0; v < 16; ++v) {
+        const double v0 = live ? __ldg(r0 + v * T) : 0.0, v1 = two ? __ldg(r1 + v * T) : 0.0;
         a0 += v0;
         a1 += v1;
-        if (!exact) s[sidx<float2>(x, k, p)] = make_float2((float)(v0 - e0), (float)(v1 - e1));
+        x[v] = make_float2((float)(v0 - e0), (float)(v1 - e1));
     }
     a0 = group_sum<BLOCK>(a0, T, red);
     a1 = group_sum<BLOCK>(a1, T, red);
     if (exact) {
         e0 = a0 / (double)N;
         e1 = a1 / (double)N;
-        for (int x = t; x < N; x += T)
-            s[sidx<float2>(x, k, p)] = make_float2(live ? (float)(__ldg(r0 + x) - e0) : 0.0f, two ? (float)(__ldg(r1 + x) - e1) : 0.0f);
+#pragma unroll
+        for (int v = 0; v < 16; ++v)
+            x[v] = make_float2(live ? (float)(__ldg(r0 + v * T) - e0) : 0.0f,
+                               two ? (float)(__ldg(r1 + v * T) - e1) : 0.0f);
     }
     if (t == 0 && live) {
         pp.spec[(size_t)j0 * pp.mp] = make_double2(a0, 0.0);
@@ -452,15 +450,93 @@ __device__ __forceinline__ void fwd_rows_r16f_dev(const PoissonPlan &pp, const d
             pp.rowmean[j1] = a1 / (double)N;
         }
     }
+    fft32::fwd_pass_store<K, 1>(x, s, t, p, pp.twf);
     __syncthreads();
-    reg_fft<false, float2>(s, k, T, t, pp.twf, p);
+    fft32::fwd_rest<K, 2>(s, t, p, pp.twf);
     if (!live) return;
     float2 *s0 = pp.specf + (size_t)j0 * pp.mp, *s1 = pp.specf + (size_t)j1 * pp.mp;
     for (int m = t; m <= N / 2; m += T) {
         if (m == 0) continue;
-        const float2 a = s[sidx<float2>(brev(m, k), k, p)], b = cconj(s[sidx<float2>(brev(N - m, k), k, p)]);
+        const float2 a = s[fft32::swz_base(brev(m, K), p)], b = cconj(s[fft32::swz_base(brev(N - m, K), p)]);
         s0[m] = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y + b.y));
         if (two) s1[m] = make_float2(0.5f * (a.y - b.y), -0.5f * (a.x - b.x));
+    }
+}
+
+// Pass C of the FP32 form: the two real rows' spectra packed as A + iB, the
+// inverse transform, psi = FP64 row mean + FP32 fluctuation / N; the last
+// radix-16 pass writes psi from registers.
+template <int BLOCK, int K>
+__device__ __forceinline__ void inv_rows_f32_k(const PoissonPlan &pp, int nxp, int ny, const double *zlo,
+                                               const double *zhi, double *__restrict__ psi, int pair_base,
+                                               float2 *sm) {
+    using S = fft32::Shape<K>;
+    constexpr int N = S::N, T = S::T;
+    const int p = threadIdx.x / T, t = threadIdx.x - p * T;
+    const int pair = pair_base + p;
+    float2 *s = sm + p * N;
+    const int j0 = 2 * pair, j1 = j0 + 1;
+    const bool live = j0 < pp.n, two = j1 < pp.n;
+    constexpr int per = BLOCK / T;
+    write_walls(psi, zlo, zhi, N, ny, nxp, pair_base / per, ((pp.n + 1) / 2 + per - 1) / per, BLOCK);
+    const float2 *s0 = pp.specf + (size_t)j0 * pp.mp, *s1 = pp.specf + (size_t)j1 * pp.mp;
+    // modes m = t + i T (i < 8) and, for t = 0, m = N/2: all loads first
+    const float2 zero = make_float2(0.0f, 0.0f);
+    float2 a[9], b[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        const int m = t + i * T;
+        const bool in = i < 8 || t == 0;
+        a[i] = (live && in && m) ? s0[m] : zero;
+        b[i] = (two && in && m) ? s1[m] : zero;
+    }
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        const int m = t + i * T;
+        if (i == 8 && t != 0) break;
+        s[fft32::swz_base(brev(m, K), p)] = make_float2(a[i].x - b[i].y, a[i].y + b[i].x);  // A + iB
+        if (m != 0 && 2 * m != N)
+            s[fft32::swz_base(brev(N - m, K), p)] = make_float2(a[i].x + b[i].y, -a[i].y + b[i].x);
+    }
+    __syncthreads();
+    fft32::inv_partial<K>(s, t, p);
+    fft32::inv_full<K, S::NF>(s, t, p, pp.twf);
+    float2 x[16];
+    fft32::inv_pass_load<K, 1>(x, s, t, p, pp.twf);
+    const double inv = 1.0 / (double)N;
+    if (pair_base == 0 && threadIdx.x == 0) *pp.rowmean_ok = 1;
+    if (live) {
+        const double mean0 = pp.spec[(size_t)j0 * pp.mp].x * inv;
+        const double mean1 = two ? pp.spec[(size_t)j1 * pp.mp].x * inv : 0.0;
+        double *p0 = psi + (size_t)(j0 + 1) * nxp + t, *p1 = psi + (size_t)(j1 + 1) * nxp + t;
+#pragma unroll
+        for (int v = 0; v < 16; ++v) {
+            p0[v * T] = mean0 + (double)x[v].x * inv;
+            if (two) p1[v * T] = mean1 + (double)x[v].y * inv;
+        }
+    }
+}
+
+// Transform sizes a block of BLOCK threads runs: 256 threads take every
+// 16 <= nx <= 4096 (several row pairs a block below 4096), 512 threads one
+// row pair of nx = 8192.
+template <int BLOCK, int K> __host__ __device__ constexpr bool r16f_fits() {
+    return BLOCK == 256 ? (K >= 4 && K <= 12) : ((1 << K) >> 4) == BLOCK;
+}
+
+#define EK_R16F_CASES(F) F(4) F(5) F(6) F(7) F(8) F(9) F(10) F(11) F(12) F(13)
+
+template <int BLOCK>
+__device__ __forceinline__ void fwd_rows_r16f_dev(const PoissonPlan &pp, const double *__restrict__ rhs, int nxp,
+                                                  int pair_base, float2 *sm, double *red) {
+    switch (pp.log2nx) {
+#define EK_CASE(K)                                                                        \
+    case K:                                                                               \
+        if constexpr (r16f_fits<BLOCK, K>()) fwd_rows_f32_k<BLOCK, K>(pp, rhs, nxp, pair_base, sm, red); \
+        break;
+        EK_R16F_CASES(EK_CASE)
+#undef EK_CASE
+        default: break;
     }
 }
 
@@ -468,39 +544,14 @@ template <int BLOCK>
 __device__ __forceinline__ void inv_rows_r16f_dev(const PoissonPlan &pp, int nxp, int ny, const double *zlo,
                                                   const double *zhi, double *__restrict__ psi, int pair_base,
                                                   float2 *sm) {
-    const int N = pp.nx, k = pp.log2nx, T = N >> 4;
-    const int p = threadIdx.x / T, t = threadIdx.x - p * T;
-    const int pair = pair_base + p;
-    float2 *s = sm + p * N;
-    const int j0 = 2 * pair, j1 = j0 + 1;
-    const bool live = j0 < pp.n, two = j1 < pp.n;
-    const float2 *s0 = pp.specf + (size_t)j0 * pp.mp, *s1 = pp.specf + (size_t)j1 * pp.mp;
-    for (int m = t; m <= N / 2; m += T) {
-        const float2 a = (live && m) ? s0[m] : make_float2(0.0f, 0.0f);
-        const float2 b = (two && m) ? s1[m] : make_float2(0.0f, 0.0f);
-        s[sidx<float2>(brev(m, k), k, p)] = make_float2(a.x - b.y, a.y + b.x);  // A + iB
-        if (m != 0 && 2 * m != N) s[sidx<float2>(brev(N - m, k), k, p)] = make_float2(a.x + b.y, -a.y + b.x);
-    }
-    __syncthreads();
-    reg_fft<true, float2>(s, k, T, t, pp.twf, p);
-    const double inv = 1.0 / (double)N;
-    if (pair_base == 0 && threadIdx.x == 0) *pp.rowmean_ok = 1;
-    if (live) {
-        const double mean0 = pp.spec[(size_t)j0 * pp.mp].x * inv;
-        const double mean1 = two ? pp.spec[(size_t)j1 * pp.mp].x * inv : 0.0;
-        double *p0 = psi + (size_t)(j0 + 1) * nxp, *p1 = psi + (size_t)(j1 + 1) * nxp;
-        for (int x = t; x < N; x += T) {
-            const float2 z = s[sidx<float2>(x, k, p)];
-            p0[x] = mean0 + (double)z.x * inv;
-            if (two) p1[x] = mean1 + (double)z.y * inv;
-        }
-    }
-    if (pair_base == 0) {
-        double *lo = psi, *hi = psi + (size_t)(ny - 1) * nxp;
-        for (int x = threadIdx.x; x < N; x += BLOCK) {
-            lo[x] = zlo[x];
-            hi[x] = zhi[x];
-        }
+    switch (pp.log2nx) {
+#define EK_CASE(K)                                                                                    \
+    case K:                                                                                           \
+        if constexpr (r16f_fits<BLOCK, K>()) inv_rows_f32_k<BLOCK, K>(pp, nxp, ny, zlo, zhi, psi, pair_base, sm); \
+        break;
+        EK_R16F_CASES(EK_CASE)
+#undef EK_CASE
+        default: break;
     }
 }
 

@@ -43,7 +43,10 @@ def test_gpu_poisson_matches_numpy(shape):
     assert np.abs(got["ey"] - ey).max() < tol * np.abs(phi).max()
 
 
-F32_SHAPES = [(16, 12), (64, 33), (512, 17), (1024, 129), (4096, 66), (8192, 18), (256, 1500)]
+# every transform length 16 ... 8192: log2 nx = 4 ... 13 covers the radix-2,
+# -4 and -8 closing passes of the row transforms
+F32_SHAPES = [(16, 12), (32, 20), (64, 33), (128, 9), (256, 1500), (512, 17), (1024, 129), (2048, 35),
+              (4096, 66), (8192, 18)]
 
 
 @pytest.mark.parametrize("shape", F32_SHAPES, ids=lambda s: f"{s[0]}x{s[1]}")
