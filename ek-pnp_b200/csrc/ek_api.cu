@@ -160,6 +160,8 @@ void refresh_chan(ek_ctx *c) {
     h.cnlo = c->wall + 4 * p.nx;
     h.cnhi = c->wall + 5 * p.nx;
     h.kref = c->kref[c->kcur];
+    h.keep_l2 = c->keep_l2;
+    c->pp.keep_l2 = c->keep_l2;
 }
 
 // Binary exponent q of a reference grid K 2^-q (values stored /36) for
@@ -462,6 +464,7 @@ int ek_create(const ek_params *p, ek_ctx **out) {
     c->plane = (size_t)p->ny * c->nxp;
     c->n = p->ny - 2;
     c->mp = round_up(p->nx / 2 + 1, 16);
+    c->keep_l2 = ek::keep_l2_fits(2 * c->plane * sizeof(double));
     const size_t pop_bytes = 27 * c->plane * pop_elem_bytes(p->storage);
     struct Alloc { void **ptr; size_t bytes; } allocs[] = {
         {(void **)&c->pops[0], pop_bytes},

@@ -285,6 +285,10 @@ int build_tables(ek_batch *b) {
     bool f32 = true;
     for (ek_ctx *c : b->ch) f32 = f32 && ek::ctx_poisson_f32(c);
     b->poisson_f32 = f32;
+    size_t field_bytes = 0;  // right-hand side + psi of the stepping channels
+    for (size_t i = 0; i < b->ch.size(); ++i)
+        if (b->active[i]) field_bytes += 2 * b->ch[i]->plane * sizeof(double);
+    for (ek_ctx *c : b->ch) c->keep_l2 = keep_l2_fits(field_bytes);
     for (size_t i = 0; i < b->ch.size(); ++i) {
         ek_ctx *c = b->ch[i];
         ek::ctx_refresh(c);

@@ -38,6 +38,7 @@ struct ek_ctx {
     bool tma_ok = false;
     int lbm_kernel = 0;                   // EK_OPT_LBM_KERNEL
     int poisson_mode = 0;                 // EK_OPT_POISSON
+    bool keep_l2 = false;                 // rhs + psi planes fit the L2 share kept for them
     int *err_dev = nullptr;               // set by bounded device waits
     ek::Rates *rates_dev = nullptr;
     ek::Rates rates{};

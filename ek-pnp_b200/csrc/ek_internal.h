@@ -16,9 +16,64 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
+
 #include "../../include/ekpnp.h"
 
 namespace ek {
+
+// Programmatic dependent launch.  A kernel started by launch_pdl may be
+// scheduled while the kernel before it in the stream is still draining; its
+// first statement is pdl_wait(), which waits for that kernel's completion
+// and the visibility of its writes, then lets the next kernel be scheduled
+// in turn.  A kernel launched the ordinary way passes pdl_wait() at once.
+// Used for a channel's one-wave row transform after the LBM step (measured
+// at 4096 x 1024: -2.6 us a step); on the many-wave LBM kernel the per-block
+// wait cost ~40 us a step, and next to the column pass's fork/join events it
+// cost more than it saved (the batched passes run many waves: not used there).
+__device__ __forceinline__ void pdl_wait() {
+#if defined(__CUDA_ARCH__)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+#endif
+}
+
+// Field-plane bytes (right-hand side + psi of every channel stepped together)
+// that the evict_last stores may pin, out of the 126 MB L2: above it the
+// planes are stored the ordinary way.
+constexpr size_t KEEP_L2_BYTES = (size_t)80 << 20;
+inline bool keep_l2_fits(size_t bytes) { return bytes <= KEEP_L2_BYTES; }
+
+// Stores of field planes that the next kernel reads back (the Poisson
+// right-hand side written by the LBM step, psi written by the inverse row
+// pass): with keep set they carry an L2 evict_last policy, so the plane
+// stays in L2 while the step's populations stream through it.
+__device__ __forceinline__ void st_field(double *p, double v, bool keep) {
+#if defined(__CUDA_ARCH__)
+    if (keep) {
+        unsigned long long pol;
+        asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+        asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(p), "d"(v), "l"(pol) : "memory");
+        return;
+    }
+#endif
+    *p = v;
+}
+
+template <typename... Exp, typename... Act>
+cudaError_t launch_pdl(void (*kern)(Exp...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Act &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, std::forward<Act>(args)...);
+}
 
 // D2Q9 velocity set in the reference numbering:  6 2 5 / 3 0 1 / 7 4 8
 __host__ __device__ constexpr int cxd(int d) {
@@ -56,6 +111,7 @@ struct Chan {
     // row y holds f - w_i * 36 * kref[s*ny + y]; every kref value is a
     // multiple of 2^-q, so 36 w_i (kref[y'] - kref[y]) is exact in FP32.
     const float *kref;
+    int keep_l2;   // right-hand side and psi planes held in L2 between kernels
 };
 
 enum Field { F_RHO = 0, F_UX, F_UY, F_CP, F_CN, F_PSI, F_EX, F_EY, F_RHS, F_COUNT };
@@ -108,6 +164,7 @@ struct PoissonPlan {
     float2 *specf;              // n x mp spectrum, FP32
     double *rowmean;            // n row means of the last solve: the offset removed before the FP32 FFT
     int *rowmean_ok;            // set by the first solve's pass C; before it pass A takes exact means
+    int keep_l2;                // psi stores ask L2 to keep the plane (see st_field)
 };
 // pass 0: row FFTs, 1: tridiagonal column solve, 2: inverse row FFTs + walls
 cudaError_t poisson_pass_f64(int pass, const PoissonPlan &pp, const Chan &c, double *fields, cudaStream_t s);
@@ -120,6 +177,7 @@ size_t poisson_smem_bytes_f64(int nx);
 // fluctuation about each row's mean; the row sums (the zero mode), its
 // column solve and the mean of psi in FP64.
 bool poisson_f32_supported(const PoissonPlan &pp);
+// Passes 0 and 2 (pass 1 is poisson_tridiag_f32_split).
 cudaError_t poisson_pass_f32_at(int pass, const PoissonPlan &pp, const Chan &c, const double *rhs, double *psi,
                                 cudaStream_t s);
 // Pass B of the FP32 form as two kernels on two streams: the FP64 zero mode
@@ -131,7 +189,8 @@ cudaError_t batch_tridiag_f32_split(const PoissonPlan *plans, const void *zero_i
 // Batched Poisson passes over many channels (ek_batch.cu builds the items):
 // pass 0/2 items int2 {channel, first row pair} (256-thread blocks, each
 // 256/(nx/16) row pairs; power-of-two nx from 16 to 4096); pass 1 items
-// int3 {channel, first mode, modes per block}.
+// int3 {channel, first mode, modes per block} (the FP64 form; the FP32 form's
+// pass 1 is batch_tridiag_f32_split).
 cudaError_t batch_poisson(int pass, const PoissonPlan *plans, const Chan *chans, double *const *fields,
                           const void *items, int nitems, cudaStream_t s, bool f32 = false);
 int poisson_tridiag_modes(int n);

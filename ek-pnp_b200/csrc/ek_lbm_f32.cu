@@ -67,6 +67,7 @@ ChanF make_chanf(const Chan &c) {
     k.cnlo = c.cnlo;
     k.cnhi = c.cnhi;
     k.kref = c.kref;
+    k.keep_l2 = c.keep_l2;
     return k;
 }
 

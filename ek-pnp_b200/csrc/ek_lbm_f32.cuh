@@ -48,6 +48,7 @@ struct ChanF {
     double inv_dy2;                    // 1/dy^2 of the wall lifting term
     const double *zlo, *zhi, *cplo, *cphi, *cnlo, *cnhi;
     const float *kref;               // per-row references / 36 (see Chan::kref)
+    int keep_l2;                     // right-hand side stores ask L2 to keep the plane
 };
 
 template <typename S> __device__ __forceinline__ float ld_pop(const S *p);
@@ -313,7 +314,7 @@ __device__ __forceinline__ void collide_shifted(const ChanF &k, float f[9], floa
         double v = k.rhs_q * qnet;
         if (y == 1) v = v - k.zlo[x] * k.inv_dy2;
         if (y == k.ny - 2) v = v - k.zhi[x] * k.inv_dy2;
-        fields[F_RHS * pl + o] = v;
+        st_field(fields + F_RHS * pl + o, v, k.keep_l2);
     }
     const float uxf = ux, uyf = uy;
     // Ion relaxation in FP64 on the FP32 deviations, rounded once on the

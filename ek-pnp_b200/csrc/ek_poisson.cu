@@ -511,8 +511,8 @@ __device__ __forceinline__ void inv_rows_f32_k(const PoissonPlan &pp, int nxp, i
         double *p0 = psi + (size_t)(j0 + 1) * nxp + t, *p1 = psi + (size_t)(j1 + 1) * nxp + t;
 #pragma unroll
         for (int v = 0; v < 16; ++v) {
-            p0[v * T] = mean0 + (double)x[v].x * inv;
-            if (two) p1[v * T] = mean1 + (double)x[v].y * inv;
+            st_field(p0 + v * T, mean0 + (double)x[v].x * inv, pp.keep_l2);
+            if (two) st_field(p1 + v * T, mean1 + (double)x[v].y * inv, pp.keep_l2);
         }
     }
 }
@@ -560,6 +560,7 @@ __device__ __forceinline__ void inv_rows_r16f_dev(const PoissonPlan &pp, int nxp
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
 fwd_rows_r16f(const PoissonPlan pp, const double *__restrict__ rhs, int nxp) {
+    pdl_wait();
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ double red[BLOCK / 32];
     fwd_rows_r16f_dev<BLOCK>(pp, rhs, nxp, blockIdx.x * (BLOCK / (pp.nx >> 4)), (float2 *)smraw, red);
@@ -689,35 +690,15 @@ __device__ __forceinline__ void tridiag_part_dev(const PoissonPlan &pp, int M, i
     tridiag_part_gen<double, double2>(pp.piv, pp.spec, pp.n, pp.nx, (size_t)pp.mp, pp.dy2, M, m_base, sh);
 }
 
-// FP32 form of pass B: block 0 solves the zero mode in FP64 (the FP64
-// spectrum's column 0, with its neighbours up to M-1 solved alongside and
-// unused); blocks 1.. solve modes 1..nx/2 in FP32, M per block.
-__device__ __forceinline__ void tridiag_part_f32_dev(const PoissonPlan &pp, int M, int block) {
-    __shared__ union {
-        TridiagSharedT<double, double2> d;
-        TridiagSharedT<float, float2> f;
-    } sh;
-    if (block == 0)
-        tridiag_part_gen<double, double2>(pp.piv, pp.spec, pp.n, pp.nx, (size_t)pp.mp, pp.dy2, M, 0, sh.d);
-    else
-        tridiag_part_gen<float, float2>(pp.pivf, pp.specf, pp.n, pp.nx, (size_t)pp.mp, (float)pp.dy2, M,
-                                        1 + (block - 1) * M, sh.f);
-}
-
 __global__ void __launch_bounds__(TB_THREADS) tridiag_part(const PoissonPlan pp, int M) {
     __shared__ TridiagShared sh;
     tridiag_part_dev(pp, M, blockIdx.x * M, sh);
 }
 
-// Two blocks per SM (64 registers): the FP32 blocks fit; the single FP64
-// zero-mode block spills a little, which costs that one block only.
-__global__ void __launch_bounds__(TB_THREADS, 2) tridiag_part_f32(const PoissonPlan pp, int M) {
-    tridiag_part_f32_dev(pp, M, blockIdx.x);
-}
-
-// Split form of the FP32 pass B: the FP64 zero-mode block on its own (no
-// register cap, so no spills), the FP32 mode blocks with two blocks per SM;
-// the caller runs the two on two streams.
+// FP32 form of pass B as two kernels that the caller runs on two streams:
+// the zero mode in FP64 (the FP64 spectrum's column 0, with its neighbours
+// up to M-1 solved alongside and unused) in one block without a register
+// cap, and modes 1..nx/2 in FP32, M per block, two blocks per SM.
 __global__ void __launch_bounds__(TB_THREADS) tridiag_zero_f64(const PoissonPlan pp, int M) {
     __shared__ TridiagShared sh;
     tridiag_part_dev(pp, M, 0, sh);
@@ -789,14 +770,6 @@ batch_tridiag_modes_f32(const PoissonPlan *__restrict__ plans, const int3 *__res
     const int3 it = items[blockIdx.x];
     const PoissonPlan pp = plans[it.x];
     tridiag_part_gen<float, float2>(pp.pivf, pp.specf, pp.n, pp.nx, (size_t)pp.mp, (float)pp.dy2, it.z, it.y, sh);
-}
-
-// items {channel, block, modes per block}: block 0 is the FP64 zero-mode block
-__global__ void __launch_bounds__(TB_THREADS, 2)
-batch_tridiag_f32(const PoissonPlan *__restrict__ plans, const int3 *__restrict__ items) {
-    const int3 it = items[blockIdx.x];
-    const PoissonPlan pp = plans[it.x];
-    tridiag_part_f32_dev(pp, it.z, it.y);
 }
 
 // Modes per block of tridiag_part for n rows, so that every segment has at
@@ -881,22 +854,18 @@ cudaError_t poisson_tridiag_f32_split(const PoissonPlan &pp, cudaStream_t s, cud
 
 cudaError_t poisson_pass_f32_at(int pass, const PoissonPlan &pp, const Chan &c, const double *rhs, double *psi,
                                 cudaStream_t s) {
-    if (!poisson_f32_supported(pp)) return cudaErrorInvalidValue;
-    if (pass == 1) {
-        const int M = tridiag_modes(pp.n);
-        tridiag_part_f32<<<1 + (pp.nx / 2 + M - 1) / M, TB_THREADS, 0, s>>>(pp, M);
-        return cudaGetLastError();
-    }
+    // pass B of this form runs through poisson_tridiag_f32_split
+    if (!poisson_f32_supported(pp) || pass == 1) return cudaErrorInvalidValue;
     int threads, per;
     r16_shape(pp.nx, &threads, &per);
     const size_t smem = (size_t)per * pp.nx * sizeof(float2);
     const int blocks = ((pp.n + 1) / 2 + per - 1) / per;
     if (threads == 256) {
-        if (pass == 0) fwd_rows_r16f<256><<<blocks, 256, smem, s>>>(pp, rhs, c.nxp);
-        else inv_rows_r16f<256><<<blocks, 256, smem, s>>>(pp, c, psi);
+        if (pass == 0) return launch_pdl(fwd_rows_r16f<256>, dim3(blocks), dim3(256), smem, s, pp, rhs, c.nxp);
+        inv_rows_r16f<256><<<blocks, 256, smem, s>>>(pp, c, psi);
     } else {
-        if (pass == 0) fwd_rows_r16f<512><<<blocks, 512, smem, s>>>(pp, rhs, c.nxp);
-        else inv_rows_r16f<512><<<blocks, 512, smem, s>>>(pp, c, psi);
+        if (pass == 0) return launch_pdl(fwd_rows_r16f<512>, dim3(blocks), dim3(512), smem, s, pp, rhs, c.nxp);
+        inv_rows_r16f<512><<<blocks, 512, smem, s>>>(pp, c, psi);
     }
     return cudaGetLastError();
 }
@@ -905,10 +874,9 @@ cudaError_t batch_poisson(int pass, const PoissonPlan *plans, const Chan *chans,
                           const void *items, int nitems, cudaStream_t s, bool f32) {
     if (nitems <= 0) return cudaSuccess;
     if (f32) {
+        if (pass == 1) return cudaErrorInvalidValue;  // runs through batch_tridiag_f32_split
         if (pass == 0)
             batch_fwd_rows_f32<<<nitems, 256, 32768, s>>>(plans, chans, fields, (const int2 *)items);
-        else if (pass == 1)
-            batch_tridiag_f32<<<nitems, TB_THREADS, 0, s>>>(plans, (const int3 *)items);
         else
             batch_inv_rows_f32<<<nitems, 256, 32768, s>>>(plans, chans, fields, (const int2 *)items);
         return cudaGetLastError();
