@@ -378,17 +378,25 @@ def run_warmstart(args, d):
     kw = dict(max_steps=cap, check=check)
     out, train = {}, {}
     modes = os.environ.get("EK_WS_MODES", "residual,direct").split(",")
+    sgs = {}
     for mode in modes:
         sg = ws.Surrogate(mode, seed=7)
         t1 = time.perf_counter()
         loss = sg.fit(trs, T[ok], iters=env_int("EK_WS_ITERS", 12000), lr=2e-3)
         train[mode] = {"seconds": time.perf_counter() - t1, "final_loss": float(loss[-200:].mean()),
                        "iterations": int(len(loss)), "gpu_launches": sg.net.launches}
-        r = ws.warm_start_run(sg, ev, **kw)
-        sg.close()
-        out[mode] = r
+        out[mode] = ws.warm_start_run(sg, ev, **kw)
+        sgs[mode] = sg
     cold = ws.cold_start_run(ev, **kw)
     best = modes[0]
+    # x-reduced relaxation (16 columns, then tiled along x), from the best
+    # network's start and from the cold start
+    xr = {}
+    for start in [a for a in os.environ.get("EK_WS_XR", "surrogate,cold").split(",") if a]:
+        xr[start] = ws.xreduced_start_run(ev, start=start, surrogate=sgs[best],
+                                          narrow_max_steps=env_int("EK_WS_NARROW_CAP", 600_000), **kw)
+    for sg in sgs.values():
+        sg.close()
     # error of each start against the channel's final state of the warm run
     errs = {}
     for mode in modes:
@@ -403,12 +411,18 @@ def run_warmstart(args, d):
         "data": "synthetic (seeded channel draws; training from the batched solver's own steady states)",
         "config": {"workload": f"warmstart-{n_eval}", "train_channels": n_train, "train_usable": int(ok.sum()),
                    "train_converged": int(np.sum(conv)), "train_gen_cap": gen_cap, "eval_channels": n_eval,
-                   "tol": 1e-8, "cap_steps": cap, "check_every": check, "storage": "f32-shifted",
+                   "tol": 1e-8, "cap_steps": cap, "narrow_cap_steps": env_int("EK_WS_NARROW_CAP", 600_000),
+                   "check_every": check, "storage": "f32-shifted",
                    "network": "4-256-256-256-512 SiLU, BF16 tcgen05, Adam"},
         "generation_s": gen_s, "training": train,
         "cold": _start_summary(cold, cap),
         "surrogate": {m: _start_summary(out[m], cap) for m in modes},
-        "wall_speedup_vs_cold": {m: cold["wall_s"] / out[m]["wall_s"] for m in modes},
+        "xreduced": {a: dict(_start_summary(r, cap), narrow_wall_s=r["narrow_wall_s"],
+                             narrow_median_steps=float(np.median(np.where(r["narrow_steps"] >= 0, r["narrow_steps"], cap))),
+                             full_steps_max=int(np.max(r["full_steps"])))
+                     for a, r in xr.items()},
+        "wall_speedup_vs_cold": dict({m: cold["wall_s"] / out[m]["wall_s"] for m in modes},
+                                     **{f"xreduced_{a}": cold["wall_s"] / r["wall_s"] for a, r in xr.items()}),
         "median_step_ratio_both_converged": (float(np.median(np.asarray(cold["steps"])[both] /
                                                              np.maximum(np.asarray(out[best]["steps"])[both], 1)))
                                              if both.any() else None),

@@ -704,6 +704,65 @@ int ek_init_equilibrium(ek_ctx *c) {
     return EK_OK;
 }
 
+extern "C++" {
+namespace {
+// dst[p][y][x] = src[p][y][x mod snx] for planes p < gridDim.z
+template <typename T>
+__global__ void tile_x_planes(const T *__restrict__ src, size_t splane, int snxp, int snx, T *__restrict__ dst,
+                              size_t dplane, int dnxp, int dnx) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= dnx) return;
+    const size_t y = blockIdx.y, pl = blockIdx.z;
+    dst[pl * dplane + y * dnxp + x] = src[pl * splane + y * snxp + x % snx];
+}
+
+template <typename T>
+cudaError_t tile_planes(const void *src, const ek_ctx *s, void *dst, const ek_ctx *d, int planes, cudaStream_t st) {
+    const dim3 g((d->p.nx + 255) / 256, d->p.ny, planes);
+    tile_x_planes<T><<<g, 256, 0, st>>>((const T *)src, s->plane, s->nxp, s->p.nx, (T *)dst, d->plane, d->nxp,
+                                        d->p.nx);
+    return cudaGetLastError();
+}
+}  // namespace
+}
+
+int ek_tile_x(ek_ctx *dst, const ek_ctx *src) {
+    if (!dst || !src || dst == src) return fail(EK_ERR_INVALID, "two distinct contexts needed");
+    if (!src->initialised) return fail(EK_ERR_INVALID, "the source holds no populations");
+    if (dst->p.ny != src->p.ny || dst->p.storage != src->p.storage || dst->p.nx % src->p.nx != 0)
+        return fail(EK_ERR_INVALID, "need the same ny and storage and a destination nx that is a multiple of the source's");
+    if (dst->device != src->device) return fail(EK_ERR_INVALID, "contexts on different devices");
+    EK_CUDA(cudaStreamSynchronize(src->stream), "source sync");
+    const int esz = (int)pop_elem_bytes(dst->p.storage);
+    cudaError_t e = esz == 8   ? tile_planes<uint64_t>(src->pops[src->cur], src, dst->pops[dst->cur], dst, 27, dst->stream)
+                    : esz == 4 ? tile_planes<uint32_t>(src->pops[src->cur], src, dst->pops[dst->cur], dst, 27, dst->stream)
+                               : tile_planes<uint16_t>(src->pops[src->cur], src, dst->pops[dst->cur], dst, 27, dst->stream);
+    EK_CUDA(e, "tile populations");
+    EK_CUDA(tile_planes<double>(src->fields, src, dst->fields, dst, F_COUNT, dst->stream), "tile fields");
+    if (dst->p.storage != EK_STORE_F64) {
+        EK_CUDA(cudaMemcpyAsync(dst->kref[dst->kcur], src->kref[src->kcur], 3 * (size_t)dst->p.ny * sizeof(float),
+                                cudaMemcpyDeviceToDevice, dst->stream),
+                "reference rows");
+        for (int q = 0; q < 3; ++q) dst->kq[q] = src->kq[q];
+    }
+    if (dst->pp.rowmean && src->pp.rowmean) {  // offsets of the FP32 Poisson form (row means: x-independent)
+        EK_CUDA(cudaMemcpyAsync(dst->pp.rowmean, src->pp.rowmean, (size_t)dst->n * sizeof(double),
+                                cudaMemcpyDeviceToDevice, dst->stream),
+                "row means");
+        EK_CUDA(cudaMemcpyAsync(dst->pp.rowmean_ok, src->pp.rowmean_ok, sizeof(int), cudaMemcpyDeviceToDevice,
+                                dst->stream),
+                "row means");
+    }
+    EK_CUDA(cudaStreamSynchronize(dst->stream), "tile");
+    dst->initialised = true;
+    dst->state_pre = src->state_pre;
+    dst->explicit_e_once = src->explicit_e_once;
+    dst->e_stale = src->e_stale;
+    dst->snap_valid = false;
+    refresh_chan(dst);
+    return EK_OK;
+}
+
 int ek_step(ek_ctx *c, int32_t nsteps) {
     if (!c || nsteps < 0) return fail(EK_ERR_INVALID, "null context or negative step count");
     if (!c->initialised) return fail(EK_ERR_INVALID, "call ek_init_equilibrium before ek_step");

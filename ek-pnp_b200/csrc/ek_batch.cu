@@ -654,6 +654,24 @@ int ek_batch_stream(const ek_batch *b, void **out) {
 // batch's current buffer parity (an even number of batch steps since they
 // were frozen).  Launches per step stay four; the work shrinks to the active
 // channels.
+int ek_batch_resync(ek_batch *b) {
+    if (!b) return ek::ctx_fail(EK_ERR_INVALID, "null batch");
+    EK_BCUDA(cudaStreamSynchronize(b->stream), "batch sync");
+    const ek_ctx *c0 = b->ch[0];
+    for (const ek_ctx *c : b->ch) {
+        if (!c->initialised) return ek::ctx_fail(EK_ERR_INVALID, "call ek_batch_init_equilibrium first");
+        if (c->cur != c0->cur || c->state_pre != c0->state_pre || c->explicit_e_once != c0->explicit_e_once)
+            return ek::ctx_fail(EK_ERR_INVALID, "the channels are not at one step parity and state");
+    }
+    b->cur = c0->cur;
+    b->state_pre = c0->state_pre;
+    b->explicit_e_once = c0->explicit_e_once;
+    for (size_t i = 0; i < b->ch.size(); ++i) b->ch_steps[i] = b->ch[i]->steps;
+    int rc = build_tables(b);  // reference rows and exponents may have changed
+    if (rc == EK_OK) rc = build_tiles(b, b->txb);
+    return rc;
+}
+
 int ek_batch_set_active(ek_batch *b, const uint8_t *mask) {
     if (!b || !mask) return ek::ctx_fail(EK_ERR_INVALID, "null argument");
     EK_BCUDA(cudaStreamSynchronize(b->stream), "batch sync");

@@ -109,6 +109,10 @@ class Batch:
                                       ms.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
         return int(chosen.value), dict(zip((64, 128, 256), ms.tolist()))
 
+    def resync(self):
+        """Adopt the channels' current states (after Channel.tile_x)."""
+        check(lib().ek_batch_resync(self._h))
+
     def set_active(self, mask):
         """Freeze (False) or step (True) each channel."""
         m = np.ascontiguousarray(np.asarray(mask, dtype=bool).astype(np.uint8))

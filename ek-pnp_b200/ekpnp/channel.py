@@ -111,6 +111,12 @@ class Channel:
     def init_equilibrium(self):
         check(lib().ek_init_equilibrium(self._h))
 
+    def tile_x(self, src):
+        """This channel's state := src's repeated along x (ek_tile_x): same ny
+        and storage, this nx a multiple of src's.  A channel inside a batch
+        is followed by Batch.resync()."""
+        check(lib().ek_tile_x(self._h, src._h))
+
     def step(self, n=1):
         check(lib().ek_step(self._h, int(n)))
 

@@ -161,6 +161,15 @@ int ek_init_poisson_boltzmann(ek_ctx *ctx, int32_t method, int32_t iterations,
  * gpu_init_equilibrium (LBM.cu:183-305). */
 int ek_init_equilibrium(ek_ctx *ctx);
 
+/* Copy the state of src into dst repeated along x: populations, fields,
+ * shifted-storage reference rows and the FP32 Poisson form's row offsets.
+ * Needs the same ny and storage and dst's nx a multiple of src's.  With
+ * walls uniform along x a channel's steady state does not depend on x, so a
+ * narrow channel relaxed to it starts a wide one there (the reference only
+ * restarts a channel of the same size, from data_end.dat).  dst keeps its
+ * step count and parameters. */
+int ek_tile_x(ek_ctx *dst, const ek_ctx *src);
+
 /* Advance nsteps coupled steps.  One step = stream_collide_save
  * (LBM.cu:307-329: collide, fluid walls, stream, ion walls) followed by
  * fast_Poisson (poisson.cu:180-208), fused as one pull-scheme LBM kernel plus
@@ -338,6 +347,10 @@ int ek_batch_autotune(ek_batch *b, int32_t steps, int32_t *chosen, double *ms3);
  * the channels that have converged).  A frozen channel rejoins only after an
  * even number of batch steps.  ek_batch_init_equilibrium activates all. */
 int ek_batch_set_active(ek_batch *b, const uint8_t *mask);
+/* Adopt the channels' current states after they were set through their own
+ * handles (ek_tile_x): all channels must be initialised and at one step
+ * parity and state; the batch steps on from there. */
+int ek_batch_resync(ek_batch *b);
 /* mask (optional, count bytes) and the number of active nodes (optional). */
 int ek_batch_active(const ek_batch *b, uint8_t *mask, int64_t *active_nodes);
 /* ek_residual of every channel: out5 gets 5 doubles per channel (u_x, c+,
