@@ -64,3 +64,16 @@ def test_pb_column_solves_the_discrete_equation():
         # rounding of the second difference of O(|zeta|) values bounds the residual
         assert np.abs(lap + src).max() <= 1e-14 * max(abs(s["zeta"]), 1.0) * 8
         assert psi[0] == psi[-1] == s["zeta"] and np.all(np.diff(psi[: len(psi) // 2]) >= 0)
+
+
+def test_xreduced_start_needs_widths_that_tile():
+    """The x-reduced run tiles 16-column states: every nx must be a multiple
+    of the narrow width (checked before any device work)."""
+    import pytest
+    from ekpnp import warmstart as ws
+    specs = [dict(nx=64, ny=32, kappa_h=4.0, zeta=-1.0, ex=1e-4, diff=0.05),
+             dict(nx=40, ny=32, kappa_h=4.0, zeta=-1.0, ex=1e-4, diff=0.05)]
+    with pytest.raises(ValueError):
+        ws.xreduced_start_run(specs, start="cold")
+    with pytest.raises(ValueError):
+        ws.xreduced_start_run(specs[:1], start="nowhere")
