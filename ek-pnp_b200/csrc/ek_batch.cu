@@ -649,11 +649,9 @@ int ek_batch_stream(const ek_batch *b, void **out) {
     return EK_OK;
 }
 
-// Channels with mask[i] == 0 stop stepping and keep their state (and step
-// count); mask[i] != 0 steps them again, which needs their state in the
-// batch's current buffer parity (an even number of batch steps since they
-// were frozen).  Launches per step stay four; the work shrinks to the active
-// channels.
+// The batch adopts its channels' current states (set through their own
+// handles, e.g. by ek_tile_x): same parity and state flags for all, step
+// counts taken from the channels, tables rebuilt.
 int ek_batch_resync(ek_batch *b) {
     if (!b) return ek::ctx_fail(EK_ERR_INVALID, "null batch");
     EK_BCUDA(cudaStreamSynchronize(b->stream), "batch sync");
@@ -672,6 +670,11 @@ int ek_batch_resync(ek_batch *b) {
     return rc;
 }
 
+// Channels with mask[i] == 0 stop stepping and keep their state (and step
+// count); mask[i] != 0 steps them again, which needs their state in the
+// batch's current buffer parity (an even number of batch steps since they
+// were frozen).  Launches per step stay the same; the work shrinks to the
+// active channels.
 int ek_batch_set_active(ek_batch *b, const uint8_t *mask) {
     if (!b || !mask) return ek::ctx_fail(EK_ERR_INVALID, "null argument");
     EK_BCUDA(cudaStreamSynchronize(b->stream), "batch sync");
