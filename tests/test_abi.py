@@ -89,3 +89,11 @@ def test_params_mapping_matches_oracle_cases():
     a = ekpnp.channel_params(256, 128, kappa_h=8.0, zeta=-2.0, ex=1e-4, diff=0.05)
     b = lattice_params(256, 128, kappa_h=8.0, zeta=-2.0, ex=1e-4, diff=0.05)
     assert a == b
+
+
+def test_state_copy_entry_points_reject_null_handles_on_host():
+    """ek_tile_x and ek_batch_resync check their handles before any CUDA call."""
+    import ekpnp
+    lib = ekpnp.lib()
+    assert lib.ek_tile_x(None, None) == 1  # EK_ERR_INVALID
+    assert lib.ek_batch_resync(None) == 1
