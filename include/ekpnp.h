@@ -305,8 +305,9 @@ int ek_diag_umax(int32_t nx, int32_t ny, const double *uy, double *out);
 /* ---- batches of independent channels ------------------------------------
  * No counterpart in the reference (one channel per run of main.cu).  A batch
  * steps many channels of different sizes and parameters in lockstep, four
- * kernel launches per step for all of them: one persistent LBM kernel over a
- * tile work-list and three batched Poisson passes.  Each channel is an ek_ctx
+ * kernel launches per step for all of them (five with the FP32 Poisson form):
+ * one persistent LBM kernel over a tile work-list and three batched Poisson
+ * passes, the FP32 form's column pass as two kernels on two streams.  Each channel is an ek_ctx
  * owned by the batch (ek_batch_channel); use it for ek_set_fields,
  * ek_set_wall_profile, ek_init_poisson_boltzmann, ek_get_fields and
  * ek_residual, but step it only through the batch.  Per channel, a batch step
@@ -342,8 +343,8 @@ int ek_batch_set_tile_width(ek_batch *b, int32_t width);
  * widths 64, 128, 256. */
 int ek_batch_autotune(ek_batch *b, int32_t steps, int32_t *chosen, double *ms3);
 /* Freeze (mask[i] == 0) or step (mask[i] != 0) each channel; a frozen
- * channel keeps its state and step count, the launches per step stay four
- * and the work shrinks to the active channels (a run to steady state freezes
+ * channel keeps its state and step count, the launches per step stay the
+ * same and the work shrinks to the active channels (a run to steady state freezes
  * the channels that have converged).  A frozen channel rejoins only after an
  * even number of batch steps.  ek_batch_init_equilibrium activates all. */
 int ek_batch_set_active(ek_batch *b, const uint8_t *mask);
