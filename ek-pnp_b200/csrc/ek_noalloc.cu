@@ -22,10 +22,21 @@
 //
 // First call on a device: the call looks up the device addresses of the arrays
 // (cudaGetSymbolAddress, once per device, with that device current) and
-// caches them.  Make that first call before any stream capture begins.
+// caches them together with the identity of the device's current context.
+// Make that first call before any stream capture begins.  After
+// cudaDeviceReset the library's module is loaded again into a new context and
+// the arrays move; the next call sees the new context and looks the addresses
+// up again (that call, too, belongs outside a stream capture).
+//
+// Errors: a launch error left pending by the caller's own earlier work is
+// cleared on entry, so it is not reported as this call's failure.  When the
+// call returns EK_ERR_CUDA, part of its work may already be queued on the
+// stream and psi, Ex and Ey are undefined.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdint>
 #include <mutex>
 
 #include "ek_internal.h"
@@ -49,16 +60,50 @@ static __device__ __align__(256) double g_na_wall[2 * NA_MAX_NX];
 struct Scratch {
     double2 *spec = nullptr, *tw = nullptr;
     double *piv = nullptr, *rhs = nullptr, *wall = nullptr;
+    unsigned long long ctx_id = 0;  // context the addresses belong to
     bool ready = false;
 };
 constexpr int NA_MAX_DEVICES = 64;
 Scratch g_scratch[NA_MAX_DEVICES];
 std::mutex g_scratch_mu;
 
-// Device addresses of the arrays for the current device (set up once).
+// Identity of the calling thread's current context (cuCtxGetId through the
+// runtime's driver entry points; the handle itself where that is missing).
+cudaError_t current_ctx_id(unsigned long long *id) {
+    typedef CUresult (*GetCurrent)(CUcontext *);
+    typedef CUresult (*GetId)(CUcontext, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = (GetCurrent)f;
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (GetId)f;
+        looked = true;
+    }
+    if (!get_current) return cudaErrorNotSupported;
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return cudaErrorDeviceUninitialized;
+    if (get_id && get_id(ctx, id) == CUDA_SUCCESS) return cudaSuccess;
+    *id = (unsigned long long)(uintptr_t)ctx;
+    return cudaSuccess;
+}
+
+// Device addresses of the arrays for the current device: looked up on the
+// first call and again whenever the device's context has changed.
 cudaError_t scratch_for(int dev, Scratch *out) {
     std::lock_guard<std::mutex> lk(g_scratch_mu);
     Scratch &s = g_scratch[dev];
+    unsigned long long id = 0;
+    const cudaError_t have = current_ctx_id(&id);
+    const bool checkable = have != cudaErrorNotSupported;  // no driver entry point: no check
+    if (s.ready && checkable && (have != cudaSuccess || s.ctx_id != id)) s.ready = false;
     if (!s.ready) {
         cudaError_t e;
         if ((e = cudaGetSymbolAddress((void **)&s.spec, g_na_spec)) != cudaSuccess) return e;
@@ -66,6 +111,9 @@ cudaError_t scratch_for(int dev, Scratch *out) {
         if ((e = cudaGetSymbolAddress((void **)&s.rhs, g_na_rhs)) != cudaSuccess) return e;
         if ((e = cudaGetSymbolAddress((void **)&s.tw, g_na_tw)) != cudaSuccess) return e;
         if ((e = cudaGetSymbolAddress((void **)&s.wall, g_na_wall)) != cudaSuccess) return e;
+        // the lookups above made the device's context current if it was not
+        if (checkable && (e = current_ctx_id(&id)) != cudaSuccess) return e;
+        s.ctx_id = id;
         s.ready = true;
     }
     *out = s;
@@ -149,6 +197,7 @@ extern "C" int ek_poisson_noalloc(const ek_params *p, const double *cp, const do
     if (p->eps == 0.0 || !std::isfinite(p->eps) || !std::isfinite(p->f_charge) || !std::isfinite(p->zeta_lo) ||
         !std::isfinite(p->zeta_hi))
         return na_fail(EK_ERR_INVALID, "non-finite eps, f_charge or wall potential, or eps == 0");
+    if (ny > 65535) return na_fail(EK_ERR_TOO_LARGE, "ek_poisson_noalloc: ny above 65535");
     if ((long long)nx * ny > EK_NOALLOC_MAX_NODES || (pow2(nx) ? nx > NA_MAX_NX : nx > 2048))
         return na_fail(EK_ERR_TOO_LARGE,
                        "ek_poisson_noalloc: nx*ny above 524288 nodes, or nx above 8192 (2048 if not a power of two)");
@@ -156,6 +205,7 @@ extern "C" int ek_poisson_noalloc(const ek_params *p, const double *cp, const do
     if ((long long)n * mp > EK_NOALLOC_MAX_NODES / 2 + 8192)
         return na_fail(EK_ERR_TOO_LARGE, "ek_poisson_noalloc: (ny-2)*(nx/2+1) spectrum above the scratch size");
     cudaStream_t s = (cudaStream_t)stream;
+    (void)cudaGetLastError();  // a launch error left by the caller's earlier work is not this call's
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess || dev < 0 || dev >= NA_MAX_DEVICES) return na_fail(EK_ERR_CUDA, "cudaGetDevice");
@@ -189,7 +239,13 @@ extern "C" int ek_poisson_noalloc(const ek_params *p, const double *cp, const do
     e = cudaMemsetAsync(sc.spec, 0, (size_t)n * mp * sizeof(double2), s);
     if (e == cudaSuccess) {
         na_tables<<<(nx + 255) / 256, 256, 0, s>>>(nx, p->zeta_lo, p->zeta_hi, sc.tw, sc.wall);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
         na_pivots<<<(mp + 127) / 128, 128, 0, s>>>(nx, n, mp, p->lx, p->dy, sc.piv);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
         na_rhs<<<rows, NA_TPB, 0, s>>>(nx, ny, p->f_charge, p->eps, p->dy, p->zeta_lo, p->zeta_hi, cp, cn, sc.rhs);
         e = cudaGetLastError();
     }
