@@ -213,11 +213,11 @@ int rebase_now(ek_ctx *c) {
     return EK_OK;
 }
 
-int copy_in(ek_ctx *c, int plane_idx, const double *src) {
+int copy_in(ek_ctx *c, int plane_idx, const double *src, cudaMemcpyKind kind = cudaMemcpyHostToDevice) {
     if (!src) return EK_OK;
     const size_t w = (size_t)c->p.nx * sizeof(double);
     EK_CUDA(cudaMemcpy2DAsync(c->fields + plane_idx * c->plane, (size_t)c->nxp * sizeof(double), src, w, w,
-                              c->p.ny, cudaMemcpyHostToDevice, c->stream),
+                              c->p.ny, kind, c->stream),
             "copy field to device");
     return EK_OK;
 }
@@ -580,15 +580,15 @@ int ek_get_params(const ek_ctx *c, ek_params *out) {
     return EK_OK;
 }
 
-int ek_set_fields(ek_ctx *c, const double *rho, const double *ux, const double *uy, const double *cp,
-                  const double *cn, const double *psi, const double *ex, const double *ey) {
+namespace {
+int set_fields_from(ek_ctx *c, const double *const src[F_RHS], cudaMemcpyKind kind) {
     if (!c) return fail(EK_ERR_INVALID, "null context");
-    if ((ex == nullptr) != (ey == nullptr)) return fail(EK_ERR_INVALID, "give both ex and ey, or neither");
-    const double *src[F_RHS] = {rho, ux, uy, cp, cn, psi, ex, ey};
+    if ((src[F_EX] == nullptr) != (src[F_EY] == nullptr)) return fail(EK_ERR_INVALID, "give both ex and ey, or neither");
     for (int k = 0; k < F_RHS; ++k) {
-        int rc = copy_in(c, k, src[k]);
+        int rc = copy_in(c, k, src[k], kind);
         if (rc != EK_OK) return rc;
     }
+    const double *ex = src[F_EX], *psi = src[F_PSI];
     if (ex) {
         c->explicit_e_once = true;
         c->e_stale = false;
@@ -597,6 +597,19 @@ int ek_set_fields(ek_ctx *c, const double *rho, const double *ux, const double *
     }
     EK_CUDA(cudaStreamSynchronize(c->stream), "set_fields sync");
     return EK_OK;
+}
+}  // namespace
+
+int ek_set_fields(ek_ctx *c, const double *rho, const double *ux, const double *uy, const double *cp,
+                  const double *cn, const double *psi, const double *ex, const double *ey) {
+    const double *src[F_RHS] = {rho, ux, uy, cp, cn, psi, ex, ey};
+    return set_fields_from(c, src, cudaMemcpyHostToDevice);
+}
+
+int ek_set_fields_device(ek_ctx *c, const double *rho, const double *ux, const double *uy, const double *cp,
+                         const double *cn, const double *psi, const double *ex, const double *ey) {
+    const double *src[F_RHS] = {rho, ux, uy, cp, cn, psi, ex, ey};
+    return set_fields_from(c, src, cudaMemcpyDeviceToDevice);
 }
 
 int ek_set_wall_profile(ek_ctx *c, const double *zlo, const double *zhi, const double *cplo,
@@ -697,6 +710,9 @@ int ek_init_equilibrium(ek_ctx *c) {
         if (rc != EK_OK) return rc;
         EK_CUDA(launch_init_shifted(c->chan, c->p.storage, c->pops[c->cur], c->fields, ee, c->stream), "init kernel");
     }
+    // the FP32 Poisson form's row offsets start over (exact row means on the
+    // first solve), so a re-initialised context repeats a fresh one bit for bit
+    if (c->pp.rowmean_ok) EK_CUDA(cudaMemsetAsync(c->pp.rowmean_ok, 0, sizeof(int), c->stream), "row offsets");
     c->initialised = true;
     c->state_pre = true;
     c->steps = 0;
@@ -770,7 +786,7 @@ int ek_step(ek_ctx *c, int32_t nsteps) {
     for (int32_t i = 0; i < nsteps; ++i) {
         const bool ee = c->explicit_e_once || (c->p.flags & EK_FLAG_EXPLICIT_E);
         const bool rebase = shifted(c) && c->rebase_every > 0 && (c->steps + 1) % c->rebase_every == 0;
-        const bool mom = every || i == nsteps - 1 || rebase;
+        const bool mom = every || (i == nsteps - 1 && c->last_moments) || rebase;
         int rc0 = timed(c, 0, "LBM step kernel", [&] {
             if (c->p.storage == EK_STORE_F64)
                 return launch_step_f64(c->chan, (const double *)c->pops[c->cur], (double *)c->pops[c->cur ^ 1],
@@ -778,7 +794,7 @@ int ek_step(ek_ctx *c, int32_t nsteps) {
             if (use_tma(c))
                 return launch_step_tma(c->chan, c->p.storage, &c->tmaps[c->cur], c->pops[c->cur],
                                        c->pops[c->cur ^ 1], c->fields, c->state_pre, ee, mom, c->err_dev,
-                                       c->stream);
+                                       c->wait_cycles, c->stream);
             return launch_step_shifted(c->chan, c->p.storage, c->pops[c->cur], c->pops[c->cur ^ 1], c->fields,
                                        c->state_pre, ee, mom, c->stream);
         });
@@ -887,6 +903,16 @@ int ek_set_option(ek_ctx *c, int32_t option, int64_t value) {
             return fail(EK_ERR_UNSUPPORTED, "the FP32 Poisson form needs shifted storage, a power-of-two nx >= 16 "
                                             "and ny <= 8194");
         c->poisson_mode = (int)value;
+        return EK_OK;
+    }
+    if (option == EK_OPT_WAIT_CYCLES) {
+        if (value < 1) return fail(EK_ERR_INVALID, "EK_OPT_WAIT_CYCLES takes cycles >= 1");
+        c->wait_cycles = (long long)value;
+        return EK_OK;
+    }
+    if (option == EK_OPT_LAST_STEP_MOMENTS) {
+        if (value < 0 || value > 1) return fail(EK_ERR_INVALID, "EK_OPT_LAST_STEP_MOMENTS takes 0 or 1");
+        c->last_moments = value != 0;
         return EK_OK;
     }
     return fail(EK_ERR_INVALID, "unknown option");

@@ -38,6 +38,8 @@ struct ek_ctx {
     bool tma_ok = false;
     int lbm_kernel = 0;                   // EK_OPT_LBM_KERNEL
     int poisson_mode = 0;                 // EK_OPT_POISSON
+    bool last_moments = true;             // EK_OPT_LAST_STEP_MOMENTS
+    long long wait_cycles = 1ll << 31;    // EK_OPT_WAIT_CYCLES
     bool keep_l2 = false;                 // rhs + psi planes fit the L2 share kept for them
     int *err_dev = nullptr;               // set by bounded device waits
     ek::Rates *rates_dev = nullptr;

@@ -146,7 +146,8 @@ cudaError_t launch_rebase(const Chan &c, int storage, void *pops, const float *k
 // map_out: a 128-byte CUtensorMap (64-byte aligned) over one population buffer.
 cudaError_t make_pop_tensor_map(int storage, const void *pops, int nxp, int ny, void *map_out);
 cudaError_t launch_step_tma(const Chan &c, int storage, const void *map, const void *src, void *dst, double *fields,
-                            bool first, bool explicit_e, bool moments, int *err, cudaStream_t s);
+                            bool first, bool explicit_e, bool moments, int *err, long long wait_cycles,
+                            cudaStream_t s);
 inline size_t pop_elem_bytes(int storage) { return storage == EK_STORE_F64 ? 8 : (storage == EK_STORE_F32 ? 4 : 2); }
 
 // ---- Poisson (ek_poisson.cu) ----

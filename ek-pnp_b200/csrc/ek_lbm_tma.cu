@@ -20,9 +20,10 @@
 // the plain kernel (collide_shifted), so both forms give bit-identical
 // results.  The two wrap columns of a channel (x = 0 pulling from nx-1 and
 // nx-1 pulling from 0) and the lower wall's row-1 pull read global memory.
-// Every mbarrier wait gives up after about 2^31 clock cycles (~1 s), sets the
-// context's error word and leaves the loop; the producer then waits (with the
-// same bound) for the copies it issued before the block exits.
+// Every mbarrier wait of the pipeline gives up after a bound (by default about
+// 2^31 clock cycles, ~1 s; EK_OPT_WAIT_CYCLES), sets the context's error word
+// and leaves the loop; the producer then waits, at the default bound, for the
+// copies it issued before the block exits.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
@@ -70,12 +71,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Wait for the phase of parity `parity` to complete, at most ~WAIT_CYCLES.
-__device__ __noinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err) {
+// Wait for the phase of parity `parity` to complete, at most `limit` cycles.
+__device__ __noinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, long long limit) {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity)) {
-        if (clock64() - t0 > WAIT_CYCLES) {
+        if (clock64() - t0 > limit) {
             atomicOr(err, 1);
             return false;
         }
@@ -97,7 +98,7 @@ template <> __device__ __forceinline__ float ld_smem<__half>(const __half *p) { 
 template <typename S, bool FIRST, bool EE>
 __global__ void __launch_bounds__(NTHREADS)
 step_tma(const __grid_constant__ CUtensorMap tsrc, const ChanF k, const S *__restrict__ src, S *__restrict__ dst,
-         double *__restrict__ fields, int *__restrict__ err, bool mom) {
+         double *__restrict__ fields, int *__restrict__ err, bool mom, long long wait_cycles) {
     using G = Geom<S>;
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *full = (uint64_t *)(smem + NSTAGE * G::STAGE_BYTES);
@@ -120,7 +121,7 @@ step_tma(const __grid_constant__ CUtensorMap tsrc, const ChanF k, const S *__res
         for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
             const int stage = it % NSTAGE;
             const uint32_t ph = (uint32_t)(it / NSTAGE) & 1u;
-            if (it >= NSTAGE && !mbar_wait(&empty[stage], ph ^ 1u, err)) break;
+            if (it >= NSTAGE && !mbar_wait(&empty[stage], ph ^ 1u, err, wait_cycles)) break;
             const int y = tile / tiles_x, x0 = (tile - y * tiles_x) * TX;
             const bool wall = y == 0 || y == k.ny - 1;
             const int ym = y == 0 ? k.ny - 1 : y - 1, yp = y + 1 == k.ny ? 0 : y + 1;
@@ -134,9 +135,10 @@ step_tma(const __grid_constant__ CUtensorMap tsrc, const ChanF k, const S *__res
                 tma_load_3d(base + plane * G::PLANE_BYTES, &tsrc, x0 - G::HALO, row, plane, &full[stage]);
             }
         }
-        // copies still in flight must land before the block exits
+        // copies still in flight must land before the block exits: waited
+        // for at the default bound whatever the pipeline's bound is
         for (int j = it > NSTAGE ? it - NSTAGE : 0; j < it; ++j)
-            mbar_wait(&full[j % NSTAGE], (uint32_t)(j / NSTAGE) & 1u, err);
+            mbar_wait(&full[j % NSTAGE], (uint32_t)(j / NSTAGE) & 1u, err, WAIT_CYCLES);
         return;
     }
 
@@ -145,7 +147,7 @@ step_tma(const __grid_constant__ CUtensorMap tsrc, const ChanF k, const S *__res
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
         const int stage = it % NSTAGE;
         const uint32_t ph = (uint32_t)(it / NSTAGE) & 1u;
-        if (!mbar_wait(&full[stage], ph, err)) break;
+        if (!mbar_wait(&full[stage], ph, err, wait_cycles)) break;
         const int y = tile / tiles_x, x0 = (tile - y * tiles_x) * TX;
         const int x = x0 + tid;
         const bool wall = y == 0 || y == k.ny - 1;
@@ -192,11 +194,12 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 template <typename S>
 cudaError_t launch_typed(const CUtensorMap &map, const ChanF &k, const void *src, void *dst, double *fields,
-                         bool first, bool ee, bool mom, int *err, int grid, cudaStream_t s) {
+                         bool first, bool ee, bool mom, int *err, long long wait_cycles, int grid,
+                         cudaStream_t s) {
     const S *a = (const S *)src;
     S *b = (S *)dst;
     const int smem = Geom<S>::SMEM_BYTES;
-#define EK_TMA(F, E) step_tma<S, F, E><<<grid, NTHREADS, smem, s>>>(map, k, a, b, fields, err, mom)
+#define EK_TMA(F, E) step_tma<S, F, E><<<grid, NTHREADS, smem, s>>>(map, k, a, b, fields, err, mom, wait_cycles)
     if (first) {
         if (ee) EK_TMA(true, true);
         else EK_TMA(true, false);
@@ -238,7 +241,8 @@ cudaError_t make_pop_tensor_map(int storage, const void *pops, int nxp, int ny, 
 }
 
 cudaError_t launch_step_tma(const Chan &c, int storage, const void *map, const void *src, void *dst, double *fields,
-                            bool first, bool explicit_e, bool moments, int *err, cudaStream_t s) {
+                            bool first, bool explicit_e, bool moments, int *err, long long wait_cycles,
+                            cudaStream_t s) {
     static bool attrs = false;
     if (!attrs) {
         cudaError_t e = set_attrs<float>();
@@ -260,8 +264,8 @@ cudaError_t launch_step_tma(const Chan &c, int storage, const void *map, const v
     int grid = sms * (per > 0 ? per : 1);
     if (grid > ntiles) grid = ntiles;
     const CUtensorMap &m = *(const CUtensorMap *)map;
-    return half ? launch_typed<__half>(m, k, src, dst, fields, first, explicit_e, moments, err, grid, s)
-                : launch_typed<float>(m, k, src, dst, fields, first, explicit_e, moments, err, grid, s);
+    return half ? launch_typed<__half>(m, k, src, dst, fields, first, explicit_e, moments, err, wait_cycles, grid, s)
+                : launch_typed<float>(m, k, src, dst, fields, first, explicit_e, moments, err, wait_cycles, grid, s);
 }
 
 }  // namespace ek

@@ -55,6 +55,7 @@ struct GemmArgs {
     bf16 *ht;       // BF16 transposed result, row stride ldht
     int ldht;
     int *err;
+    long long wait_cycles;  // bound of each wait for the MMAs of a K chunk
 };
 
 __device__ __forceinline__ float silu(float z) { return z / (1.0f + expf(-z)); }
@@ -113,7 +114,7 @@ __global__ void __launch_bounds__(128) mlp_gemm(const GemmArgs g) {
             }
             ek::tc::mma_commit(&bar);
         }
-        const bool ok = ek::tc::mbar_wait_bounded(&bar, phase);
+        const bool ok = ek::tc::mbar_wait_bounded(&bar, phase, g.wait_cycles);
         phase ^= 1;
         failed = __syncthreads_or(!ok) != 0;  // also: the tiles may be overwritten
         ek::tc::fence_after_sync();
@@ -121,8 +122,9 @@ __global__ void __launch_bounds__(128) mlp_gemm(const GemmArgs g) {
     }
     if (failed) {
         if (tid == 0) atomicOr(g.err, 1);
-        // give MMAs still in flight one more bounded wait before freeing TMEM
-        ek::tc::mbar_wait_bounded(&bar, phase);
+        // MMAs still in flight get one more wait, at the default bound
+        // whatever the pipeline's, before the tensor memory is freed
+        ek::tc::mbar_wait_bounded(&bar, phase, ek::tc::WAIT_CYCLES_DEFAULT);
     } else {
         const int row = m0 + warp * 32 + lane;
         const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
@@ -283,6 +285,7 @@ struct ek_mlp {
     std::mt19937_64 rng;
     std::vector<int> perm;          // permutation of the current epoch
     int *err = nullptr;
+    long long wait_cycles = ek::tc::WAIT_CYCLES_DEFAULT;
     cudaGraphExec_t graph = nullptr;
     float graph_lr = -1.0f;
     int64_t launches = 0;
@@ -307,8 +310,10 @@ cudaError_t gemm(const GemmArgs &a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-GemmArgs args(const bf16 *a, int lda, const bf16 *b, int ldb, int m, int n, int k, int *err) {
+GemmArgs args(const bf16 *a, int lda, const bf16 *b, int ldb, int m, int n, int k, int *err,
+              long long wait_cycles = ek::tc::WAIT_CYCLES_DEFAULT) {
     GemmArgs g{};
+    g.wait_cycles = wait_cycles;
     g.a = a;
     g.lda = lda;
     g.b = b;
@@ -327,7 +332,7 @@ int forward(ek_mlp *q) {
     const bf16 *in = q->x;
     int ldin = INP;
     for (int l = 0; l < 3; ++l) {
-        GemmArgs a = args(in, ldin, q->wb[l], DIM_IN[l], B, HID, DIM_IN[l], q->err);
+        GemmArgs a = args(in, ldin, q->wb[l], DIM_IN[l], B, HID, DIM_IN[l], q->err, q->wait_cycles);
         a.bias = q->p + q->off_b[l];
         a.z = q->z[l];
         a.ldz = HID;
@@ -339,7 +344,7 @@ int forward(ek_mlp *q) {
         in = q->h[l];
         ldin = HID;
     }
-    GemmArgs a = args(in, HID, q->wb[3], HID, B, OUT, HID, q->err);
+    GemmArgs a = args(in, HID, q->wb[3], HID, B, OUT, HID, q->err, q->wait_cycles);
     a.bias = q->p + q->off_b[3];
     a.c = q->y;
     a.ldc = OUT;
@@ -356,7 +361,7 @@ int backward(ek_mlp *q, bool counted) {
     EK_MCUDA(cudaGetLastError(), "loss kernel");
     // layer 3: dW3 = dY^T H2, dZ2 = (dY W3) * silu'(Z2)
     {
-        GemmArgs a = args(q->dyt, B, q->ht[2], B, OUT, HID, B, q->err);
+        GemmArgs a = args(q->dyt, B, q->ht[2], B, OUT, HID, B, q->err, q->wait_cycles);
         a.c = q->g + q->off_w[3];
         a.ldc = HID;
         EK_MCUDA(gemm<EPI_F32>(a, q->stream), "weight-gradient GEMM");
@@ -365,7 +370,7 @@ int backward(ek_mlp *q, bool counted) {
     int ldup = OUT;
     for (int l = 2; l >= 0; --l) {
         // dZ_l = (dZ_{l+1} W_{l+1}) * silu'(Z_l)
-        GemmArgs a = args(up, ldup, q->wt[l + 1], DIM_OUT[l + 1], B, HID, DIM_OUT[l + 1], q->err);
+        GemmArgs a = args(up, ldup, q->wt[l + 1], DIM_OUT[l + 1], B, HID, DIM_OUT[l + 1], q->err, q->wait_cycles);
         a.z = q->z[l];
         a.ldz = HID;
         a.h = q->dz[l];
@@ -375,7 +380,7 @@ int backward(ek_mlp *q, bool counted) {
         EK_MCUDA(gemm<EPI_BWD_HIDDEN>(a, q->stream), "backward GEMM");
         // dW_l = dZ_l^T H_{l-1} (H_{-1} = X)
         const bf16 *hin_t = l > 0 ? q->ht[l - 1] : q->xt;
-        GemmArgs w = args(q->dzt[l], B, hin_t, B, HID, DIM_IN[l], B, q->err);
+        GemmArgs w = args(q->dzt[l], B, hin_t, B, HID, DIM_IN[l], B, q->err, q->wait_cycles);
         w.c = q->g + q->off_w[l];
         w.ldc = DIM_IN[l];
         EK_MCUDA(gemm<EPI_F32>(w, q->stream), "weight-gradient GEMM");
@@ -724,6 +729,58 @@ int ek_mlp_forward(ek_mlp *q, const float *x, int64_t n, float *y) {
 int ek_mlp_launch_count(const ek_mlp *q, int64_t *out) {
     if (!q || !out) return ek::ctx_fail(EK_ERR_INVALID, "null argument");
     *out = q->launches;
+    return EK_OK;
+}
+
+int ek_mlp_set_wait_cycles(ek_mlp *q, int64_t cycles) {
+    if (!q || cycles < 1) return ek::ctx_fail(EK_ERR_INVALID, "need a network and cycles >= 1");
+    EK_MCUDA(cudaStreamSynchronize(q->stream), "wait bound");
+    if (q->graph) cudaGraphExecDestroy(q->graph);  // it holds the old bound
+    q->graph = nullptr;
+    q->wait_cycles = cycles;
+    return EK_OK;
+}
+
+}  // extern "C"
+
+namespace {
+// One block of 64 threads: thread 0 waits, at most `cycles`, on an mbarrier
+// that expects one arrival; thread 32 (another warp) arrives only if
+// `arrive`.  out[0] = 1 if the wait gave up, out[1] = 1 when thread 0 is done.
+__global__ void __launch_bounds__(64) wait_selftest(long long cycles, int arrive, int *out) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        ek::tc::mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 32 && arrive)
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(ek::tc::smem_u32(&bar)) : "memory");
+    if (threadIdx.x == 0) {
+        const bool ok = ek::tc::mbar_wait_bounded(&bar, 0, cycles);
+        out[0] = ok ? 0 : 1;
+        out[1] = 1;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+int ek_wait_selftest(int64_t cycles, int32_t arrive) {
+    if (cycles < 1) return ek::ctx_fail(EK_ERR_INVALID, "need cycles >= 1");
+    int *out = nullptr;
+    EK_MCUDA(cudaMalloc(&out, 2 * sizeof(int)), "self-test word");
+    cudaError_t e = cudaMemset(out, 0, 2 * sizeof(int));
+    if (e == cudaSuccess) {
+        wait_selftest<<<1, 64>>>((long long)cycles, arrive ? 1 : 0, out);
+        e = cudaGetLastError();
+    }
+    int h[2] = {0, 0};
+    if (e == cudaSuccess) e = cudaMemcpy(h, out, sizeof(h), cudaMemcpyDeviceToHost);
+    cudaFree(out);
+    EK_MCUDA(e, "self-test kernel");
+    if (h[1] != 1) return ek::ctx_fail(EK_ERR_CUDA, "self-test kernel did not finish");
+    if (h[0]) return ek::ctx_fail(EK_ERR_TIMEOUT, "the bounded wait gave up (as asked: nothing arrived)");
     return EK_OK;
 }
 

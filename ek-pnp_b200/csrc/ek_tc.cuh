@@ -32,12 +32,15 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Wait for the phase of parity `parity`, giving up after ~2^31 cycles (~1 s).
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+// Default bound of a wait: ~2^31 SM clock cycles (about a second).
+constexpr long long WAIT_CYCLES_DEFAULT = 1ll << 31;
+// Wait for the phase of parity `parity`, giving up after `limit` cycles.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,
+                                                  long long limit = WAIT_CYCLES_DEFAULT) {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity))
-        if (clock64() - t0 > (1ll << 31)) return false;
+        if (clock64() - t0 > limit) return false;
     return true;
 }
 

@@ -68,6 +68,9 @@ _SIGS = {
     "ek_set_stream": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "ek_get_params": ([ctypes.c_void_p, _P(EkParams)], ctypes.c_int),
     "ek_set_fields": ([ctypes.c_void_p] + [_dp] * 8, ctypes.c_int),
+    "ek_set_fields_device": ([ctypes.c_void_p] + [ctypes.c_void_p] * 8, ctypes.c_int),
+    "ek_mlp_set_wait_cycles": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int),
+    "ek_wait_selftest": ([ctypes.c_int64, ctypes.c_int32], ctypes.c_int),
     "ek_set_wall_profile": ([ctypes.c_void_p] + [_dp] * 6, ctypes.c_int),
     "ek_init_equilibrium": ([ctypes.c_void_p], ctypes.c_int),
     "ek_tile_x": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),

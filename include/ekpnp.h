@@ -133,6 +133,11 @@ int ek_get_params(const ek_ctx *ctx, ek_params *out);
 int ek_set_fields(ek_ctx *ctx, const double *rho, const double *ux,
                   const double *uy, const double *cp, const double *cn,
                   const double *psi, const double *ex, const double *ey);
+/* Same as ek_set_fields from device buffers of nx*ny doubles (index nx*y + x),
+ * e.g. the caller's own rho_gpu, charge_gpu, ... of main.cu:102-110. */
+int ek_set_fields_device(ek_ctx *ctx, const double *rho, const double *ux,
+                         const double *uy, const double *cp, const double *cn,
+                         const double *psi, const double *ex, const double *ey);
 
 /* Per-x wall potential and wall concentrations (nx doubles each, any may be
  * NULL to keep the uniform value).  Extends the uniform voltage/charge0
@@ -191,14 +196,27 @@ int ek_set_rebase_interval(ek_ctx *ctx, int32_t steps);
  * (producer warp + mbarrier ring of tensor copies).  Both forms give
  * bit-identical results.  Returns EK_ERR_UNSUPPORTED for a form that this
  * context cannot run. */
-enum { EK_OPT_LBM_KERNEL = 1, EK_OPT_POISSON = 2 };
+enum { EK_OPT_LBM_KERNEL = 1, EK_OPT_POISSON = 2, EK_OPT_LAST_STEP_MOMENTS = 3, EK_OPT_WAIT_CYCLES = 4 };
 /* EK_OPT_POISSON selects the arithmetic of the Poisson solve (ek_step and
  * ek_poisson): 0 = automatic (the FP32 form for FP32/FP16 storage where it
  * applies, FP64 otherwise), 1 = FP64, 2 = FP32 form: row FFTs and column
  * solves of the x-modes >= 1 in FP32 on the fluctuation about each row's
  * mean, the zero mode (row sums, its column solve, the mean of psi) in FP64.
  * The FP32 form needs shifted storage, a power-of-two nx >= 16 and
- * ny <= 8194 (EK_ERR_UNSUPPORTED otherwise). */
+ * ny <= 8194 (EK_ERR_UNSUPPORTED otherwise).
+ * EK_OPT_LAST_STEP_MOMENTS: 1 (default) = the last step of every ek_step call
+ * writes the moments rho, ux, uy, c+, c- to the field planes; 0 = only the
+ * steps that need them anyway (re-basing, EK_FLAG_MOMENTS_EVERY_STEP) write
+ * them, and the planes keep the moments of the last step that did.  psi and
+ * E follow every step either way.  A caller that steps one step per call and
+ * reads the moments only now and then (the reference's loop, main.cu:190-233)
+ * sets 0 and switches to 1 for the steps whose moments it reads; the choice
+ * never changes the arithmetic of a step.
+ * EK_OPT_WAIT_CYCLES: bound, in SM clock cycles (>= 1), of each wait of the
+ * TMA-fed kernel's pipeline (default 2^31, about a second).  A wait that runs
+ * out sets the context's error word; the producer still waits, at the
+ * default bound, for the copies it issued; the next ek_sync or
+ * ek_get_fields returns EK_ERR_TIMEOUT and the context stays usable. */
 int ek_set_option(ek_ctx *ctx, int32_t option, int64_t value);
 
 /* Poisson solve for the current c+, c- moments, then psi and E:
@@ -247,11 +265,15 @@ int ek_field_pointers(ek_ctx *ctx, double **out8, int32_t *pitch);
  * buffer in device arrays built into the library (10.9 MB per GPU, held until
  * the process exits).  cp, cn, psi, ex, ey: device arrays of nx*ny doubles,
  * index nx*y + x.  Uses nx, ny, dx, dy, lx, eps, f_charge, zeta_lo, zeta_hi of p.
- * Limit: nx*ny <= 524288 nodes (nx a power of two <= 8192, or nx <= 2048);
- * larger channels return EK_ERR_TOO_LARGE.  All calls on a GPU share the
- * scratch: calls that overlap on the GPU race, so order them on one stream.
- * The first call on a device looks up the scratch addresses; make it before
- * any stream capture.  stream: a cudaStream_t, NULL for the legacy stream. */
+ * Limit: nx*ny <= 524288 nodes (nx a power of two <= 8192, or nx <= 2048)
+ * and ny <= 65535; larger channels return EK_ERR_TOO_LARGE before any work
+ * is queued.  All calls on a GPU share the scratch: calls that overlap on the
+ * GPU race, so order them on one stream.  The first call on a device looks up
+ * the scratch addresses; make it before any stream capture.  After
+ * cudaDeviceReset the next call looks them up again (also outside a capture).
+ * A launch error pending from the caller's earlier work is cleared on entry;
+ * on EK_ERR_CUDA part of the call may be queued and psi, ex, ey are undefined.
+ * stream: a cudaStream_t, NULL for the legacy stream. */
 int ek_poisson_noalloc(const ek_params *p, const double *cp, const double *cn,
                        double *psi, double *ex, double *ey, void *stream);
 
@@ -388,6 +410,17 @@ int ek_mlp_gradients(ek_mlp *m, const float *x, const float *t, float *grads, do
 /* y (n x 512) = network(x (n x 4)), host arrays. */
 int ek_mlp_forward(ek_mlp *m, const float *x, int64_t n, float *y);
 int ek_mlp_launch_count(const ek_mlp *m, int64_t *out);
+/* Bound, in SM clock cycles (>= 1), of each wait for the tensor cores inside
+ * the network's GEMMs (default 2^31, about a second).  A wait that runs out
+ * makes the call return EK_ERR_TIMEOUT; MMAs still in flight are waited for
+ * at the default bound before the tensor memory is freed. */
+int ek_mlp_set_wait_cycles(ek_mlp *m, int64_t cycles);
+/* Device self-test of the bounded wait used by the GEMMs: one thread waits,
+ * at most `cycles`, on a shared-memory barrier that another thread completes
+ * only if arrive != 0.  Returns EK_OK when the wait saw the arrival and
+ * EK_ERR_TIMEOUT when it gave up; either way the kernel ends and the device
+ * stays usable. */
+int ek_wait_selftest(int64_t cycles, int32_t arrive);
 /* C (m x n, FP32, row stride ldc) = A (m x k) * B (n x k)^T on the tensor
  * cores; A, B BF16 (uint16 bit patterns), device pointers 16-byte aligned;
  * m a multiple of 128, n a multiple of 16 (of 128 above 128), k a multiple of

@@ -92,7 +92,7 @@ def patch_sources(src: dict, p: dict, steps: int) -> dict:
         h = _sub1(h, r"(\ndouble\s+" + name + r"\s*=\s*)[^;]+;", r"\g<1>" + _lit(v) + ";", name)
     src["LBM.h"] = h
 
-    if p["flags"] & FLAG_FORCE:
+    if p["flags"] & FLAG_FORCE and "LBM.cu" in src:
         src["LBM.cu"] = _sub1(src["LBM.cu"], r"double (force[xy]m?) = 0;//\s*([^;\n]+);",
                               r"double \1 = \2;", "electric body force", count=4)
 
@@ -138,8 +138,67 @@ def build_case(name: str, force: bool = False) -> str:
     return exe
 
 
+# The drop-in build: the reference's main.cu, LBM.h, seconds.cpp and
+# seconds.h (patched exactly as for build_case: sizes, constants, dump block)
+# with this project's shim LBM.cu and poisson.cu in place of the reference's,
+# linked against libekpnp.so.  Output oracle/_ref/<case>/ekshim.
+SHIM_DIR = os.path.join(os.path.dirname(HERE), "ek-pnp_b200", "shim")
+LIB_DIR = os.path.join(os.path.dirname(HERE), "ek-pnp_b200", "ekpnp")
+INCLUDE_DIR = os.path.join(os.path.dirname(HERE), "include")
+SHIM_SOURCES = ("LBM.cu", "poisson.cu")
+
+
+def build_shim_case(name: str, force: bool = False) -> str:
+    p, seed, steps = CASES[name]
+    out = os.path.join(OUT_DIR, name)
+    exe = os.path.join(out, "ekshim")
+    meta = os.path.join(out, "shim.json")
+    shim = {}
+    for f in SHIM_SOURCES:
+        with open(os.path.join(SHIM_DIR, f)) as fh:
+            shim[f] = fh.read()
+    header = open(os.path.join(INCLUDE_DIR, "ekpnp.h")).read()
+    want = dict(params=p, seed=seed, steps=steps, shim=shim, header=header)
+    if not force and os.path.exists(exe) and os.path.exists(meta):
+        with open(meta) as fh:
+            if json.load(fh) == json.loads(json.dumps(want)):
+                return exe
+    if not os.path.isdir(REF_DIR):
+        raise FileNotFoundError(f"reference checkout not found at {REF_DIR}")
+    if not os.path.exists(os.path.join(LIB_DIR, "libekpnp.so")):
+        raise FileNotFoundError("libekpnp.so missing: build the library first")
+    src = {}
+    for f in ("main.cu", "LBM.h", "seconds.cpp", "seconds.h"):
+        with open(os.path.join(REF_DIR, f), encoding="latin-1") as fh:
+            src[f] = fh.read()
+    src = patch_sources(src, p, steps)
+    os.makedirs(out, exist_ok=True)
+    with tempfile.TemporaryDirectory(prefix="ekshim_") as tmp:
+        for f, text in src.items():
+            with open(os.path.join(tmp, f), "w", encoding="latin-1") as fh:
+                fh.write(text)
+        for f, text in shim.items():
+            with open(os.path.join(tmp, f), "w") as fh:
+                fh.write(text)
+        rpath = "$ORIGIN/" + os.path.relpath(LIB_DIR, out)
+        cmd = [NVCC, "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-w", "-I" + INCLUDE_DIR,
+               f"-DEKPNP_SHIM_FORCE={1 if p['flags'] & FLAG_FORCE else 0}",
+               "main.cu", "seconds.cpp", "-L" + LIB_DIR, "-lekpnp", "-lcufft",
+               "-Xlinker", "-rpath," + rpath, "-o", exe]
+        r = subprocess.run(cmd, cwd=tmp, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("drop-in build failed:\n" + r.stdout + r.stderr)
+    with open(meta, "w") as fh:
+        json.dump(want, fh)
+    return exe
+
+
 def build_all(names=None) -> list:
     return [build_case(n) for n in (names or CASES)]
+
+
+def build_all_shims(names=None) -> list:
+    return [build_shim_case(n) for n in (names or CASES)]
 
 
 def available() -> bool:
@@ -147,5 +206,5 @@ def available() -> bool:
 
 
 if __name__ == "__main__":
-    for path in build_all(sys.argv[1:] or None):
+    for path in build_all(sys.argv[1:] or None) + build_all_shims(sys.argv[1:] or None):
         print(path)

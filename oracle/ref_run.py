@@ -31,10 +31,12 @@ def write_restart(path, f):
     np.savetxt(path, cols, fmt="%.17g")
 
 
-def run_case(name, init, workdir, timeout=900):
-    """Run case `name` from the fields `init`; return (fields, info)."""
+def run_case(name, init, workdir, timeout=900, binary="ekref"):
+    """Run case `name` from the fields `init`; return (fields, info).
+    binary "ekref" is the patched reference build, "ekshim" the reference's
+    main.cu over this project's drop-in LBM.cu/poisson.cu and libekpnp."""
     p, _, _ = CASES[name]
-    exe = os.path.join(HERE, "_ref", name, "ekref")
+    exe = os.path.join(HERE, "_ref", name, binary)
     if not os.path.exists(exe):
         raise FileNotFoundError(exe + " (build it with oracle/ref_build.py)")
     os.makedirs(workdir, exist_ok=True)
