@@ -204,10 +204,15 @@ def run_ours(args, d):
     # ---- roofline of the dominant kernel (the fused LBM step) ----
     lbm_ms, lbm_n = prof["lbm"]
     per_launch_s = lbm_ms / max(lbm_n, 1) / 1e3
-    bytes_node = 54 * POP_BYTES[args.storage] + 16  # 27 pops in + 27 out, psi in, rhs out (FP64)
+    # 27 pops in + 27 out, psi in, right-hand side out: FP64 planes for FP64
+    # storage, FP32 planes (psi and rhs about FP64 row constants) for shifted
+    fld = 8 if args.storage == "f64" else 4
+    bytes_node = 54 * POP_BYTES[args.storage] + 2 * fld
     achieved = nn * bytes_node / per_launch_s / 1e9
     peak, peak_kind = measured_peak_gbs()
     traffic = ncu_traffic(args.workload, args.storage)
+    # whole step at B_node = 54 s_pop + 8 s_fld (LBM, Poisson passes A, B, C)
+    step_bytes = 54 * POP_BYTES[args.storage] + 8 * fld
     step_ms = ms / args.steps
     shares = {k: round(v[0] / max(sum(x[0] for x in prof.values()), 1e-12), 4) for k, v in prof.items()}
     ch.close()
@@ -260,7 +265,14 @@ def run_ours(args, d):
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "fused LBM step", "bytes_per_node": bytes_node,
                          "launch_ms": per_launch_s * 1e3,
-                         "timing": "CUDA events around each launch, second pass of the same K steps"},
+                         "timing": "CUDA events around each launch, second pass of the same K steps",
+                         "traffic_source": (f"profiles/lbm_{args.storage}_{args.workload}.json: ncu "
+                                            "dram__bytes_read.sum + dram__bytes_write.sum of this kernel on "
+                                            "this workload (a separate capture, not this run)")
+                         if traffic is not None else None},
+            "step_roofline": {"bytes_per_node": step_bytes, "achieved": value * 1e6 * step_bytes / 1e9,
+                              "unit": "GB/s", "frac": value * 1e6 * step_bytes / 1e9 / peak,
+                              "basis": "54 s_pop + 8 s_fld per node and step (LBM + Poisson passes)"},
             "step_breakdown": {"ms_per_step": step_ms,
                                "kernel_ms": {k: v[0] / max(v[1], 1) for k, v in prof.items()},
                                "share": shares},
@@ -388,11 +400,15 @@ def run_warmstart(args, d):
         out[mode] = ws.warm_start_run(sg, ev, **kw)
         sgs[mode] = sg
     cold = ws.cold_start_run(ev, **kw)
+    # the method without the network: the Newton Poisson-Boltzmann ions and
+    # potential with the electro-osmotic velocity (the reference's own start,
+    # LBM.cu:95-145, solved to convergence, plus the Helmholtz-Smoluchowski flow)
+    phys = ws.physics_start_run(ev, **kw)
     best = modes[0]
     # x-reduced relaxation (16 columns, then tiled along x), from the best
     # network's start and from the cold start
     xr = {}
-    for start in [a for a in os.environ.get("EK_WS_XR", "surrogate,cold").split(",") if a]:
+    for start in [a for a in os.environ.get("EK_WS_XR", "surrogate,physics,cold").split(",") if a]:
         xr[start] = ws.xreduced_start_run(ev, start=start, surrogate=sgs[best],
                                           narrow_max_steps=env_int("EK_WS_NARROW_CAP", 600_000), **kw)
     for sg in sgs.values():
@@ -416,13 +432,17 @@ def run_warmstart(args, d):
                    "network": "4-256-256-256-512 SiLU, BF16 tcgen05, Adam"},
         "generation_s": gen_s, "training": train,
         "cold": _start_summary(cold, cap),
+        "physics": _start_summary(phys, cap),
         "surrogate": {m: _start_summary(out[m], cap) for m in modes},
         "xreduced": {a: dict(_start_summary(r, cap), narrow_wall_s=r["narrow_wall_s"],
                              narrow_median_steps=float(np.median(np.where(r["narrow_steps"] >= 0, r["narrow_steps"], cap))),
                              full_steps_max=int(np.max(r["full_steps"])))
                      for a, r in xr.items()},
         "wall_speedup_vs_cold": dict({m: cold["wall_s"] / out[m]["wall_s"] for m in modes},
+                                     physics=cold["wall_s"] / phys["wall_s"],
                                      **{f"xreduced_{a}": cold["wall_s"] / r["wall_s"] for a, r in xr.items()}),
+        "wall_speedup_vs_physics": dict({m: phys["wall_s"] / out[m]["wall_s"] for m in modes},
+                                        **{f"xreduced_{a}": phys["wall_s"] / r["wall_s"] for a, r in xr.items()}),
         "median_step_ratio_both_converged": (float(np.median(np.asarray(cold["steps"])[both] /
                                                              np.maximum(np.asarray(out[best]["steps"])[both], 1)))
                                              if both.any() else None),

@@ -84,6 +84,9 @@ void free_ctx(ek_ctx *c) {
     cudaFree(c->rates_dev);
     cudaFree(c->kref[0]);
     cudaFree(c->kref[1]);
+    cudaFree(c->kwall);
+    cudaFree(c->wdelta);
+    cudaFree(c->lift);
     cudaFree(c->err_dev);
     cudaFree(c->pp.tw);
     cudaFree(c->pp.piv);
@@ -93,6 +96,9 @@ void free_ctx(ek_ctx *c) {
     cudaFree(c->pp.specf);
     cudaFree(c->pp.rowmean);
     cudaFree(c->pp.rowmean_ok);
+    cudaFree(c->pp.rhsf);
+    cudaFree(c->pp.psif);
+    cudaFree(c->pp.psim);
     for (auto &pr : c->ev_pool) {
         cudaEventDestroy(pr.first);
         cudaEventDestroy(pr.second);
@@ -160,8 +166,21 @@ void refresh_chan(ek_ctx *c) {
     h.cnlo = c->wall + 4 * p.nx;
     h.cnhi = c->wall + 5 * p.nx;
     h.kref = c->kref[c->kcur];
+    h.kwall = c->kwall;
+    h.wdelta = c->wdelta;
+    h.rhsf = c->pp.rhsf;
+    h.psif = c->pp.psif;
+    h.psim = c->pp.psim;
+    h.lift = c->lift;
     h.keep_l2 = c->keep_l2;
     c->pp.keep_l2 = c->keep_l2;
+    double zl = 0.0, zh = 0.0;  // x-means of the wall potentials (psim of the wall rows)
+    for (int x = 0; x < p.nx; ++x) {
+        zl += c->wall_host[x];
+        zh += c->wall_host[(size_t)p.nx + x];
+    }
+    c->pp.zlo_mean = zl / p.nx;
+    c->pp.zhi_mean = zh / p.nx;
 }
 
 // Binary exponent q of a reference grid K 2^-q (values stored /36) for
@@ -174,6 +193,23 @@ int ref_exponent(double vmax) {
 }
 
 int shifted(const ek_ctx *c) { return c->p.storage != EK_STORE_F64; }
+
+// Shifted storage: the x-fluctuation of the wall lifting, (zeta(x) -
+// zeta_mean)/dy^2 per wall, from the host copy of the wall profiles (the
+// x-means themselves are refreshed by refresh_chan).
+int upload_lift(ek_ctx *c) {
+    if (!shifted(c)) return EK_OK;
+    const int nx = c->p.nx;
+    const double inv_dy2 = 1.0 / (c->p.dy * c->p.dy);
+    std::vector<float> l(2 * (size_t)nx);
+    for (int x = 0; x < nx; ++x) {
+        l[x] = (float)((c->wall_host[x] - c->pp.zlo_mean) * inv_dy2);
+        l[(size_t)nx + x] = (float)((c->wall_host[(size_t)nx + x] - c->pp.zhi_mean) * inv_dy2);
+    }
+    EK_CUDA(cudaMemcpyAsync(c->lift, l.data(), l.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream), "lift");
+    EK_CUDA(cudaStreamSynchronize(c->stream), "lift");
+    return EK_OK;
+}
 
 // The TMA-fed form runs four compute warps per block; on the measured B200
 // the node update is issue-bound and the plain form (more resident warps) is
@@ -274,11 +310,28 @@ int side_stream(ek_ctx *c) {
     return EK_OK;
 }
 
-int poisson_now(ek_ctx *c) {
+// The Poisson solve of a step (or of a solve outside the step when
+// from_moments: the right-hand side from the c+, c- moments).  FP64 storage:
+// the FP64 passes on the FP64 planes.  Shifted storage, FP32 form: the passes
+// read rhsf and write psif/psim, and the FP64 psi plane too when write_f64.
+// Shifted storage, FP64 passes: the FP64 right-hand side composed from rhsf,
+// then psif/psim split from the FP64 psi.
+int poisson_now(ek_ctx *c, bool write_f64, bool from_moments = false) {
+    const bool sh = shifted(c);
     const bool f32 = ek::ctx_poisson_f32(c);
+    if (c->p.flags & EK_FLAG_EXPLICIT_E) write_f64 = true;  // the E planes follow psi every step
     if (f32) {
         int rc = side_stream(c);
         if (rc != EK_OK) return rc;
+    }
+    double *rhs = c->fields + F_RHS * c->plane, *psi = c->fields + F_PSI * c->plane;
+    if (from_moments) {
+        if (f32) EK_CUDA(launch_rhsf_from_moments(c->pp, c->chan, c->fields, c->stream), "rhs kernel");
+        else EK_CUDA(launch_rhs_from_moments_f64(c->chan, c->fields, c->stream), "rhs kernel");
+        ++c->launches;
+    } else if (sh && !f32) {
+        EK_CUDA(launch_compose_rhs(c->pp, c->chan, rhs, c->stream), "rhs kernel");
+        ++c->launches;
     }
     for (int pass = 0; pass < 3; ++pass) {
         // FP32 form, pass B: FP64 zero mode on the side stream beside the
@@ -288,19 +341,33 @@ int poisson_now(ek_ctx *c) {
             c, 1 + pass, "poisson kernel",
             [&] {
                 if (split) return poisson_tridiag_f32_split(c->pp, c->stream, c->side, c->fork, c->join);
-                return f32 ? poisson_pass_f32_at(pass, c->pp, c->chan, c->fields + F_RHS * c->plane,
-                                                 c->fields + F_PSI * c->plane, c->stream)
+                return f32 ? poisson_pass_f32(pass, c->pp, c->chan, psi, write_f64, c->stream)
                            : poisson_pass_f64(pass, c->pp, c->chan, c->fields, c->stream);
             },
             split ? 2 : 1);
         if (rc != EK_OK) return rc;
     }
+    if (sh && !f32) {
+        EK_CUDA(launch_split_psi(c->pp, c->chan, psi, c->stream), "split psi");
+        ++c->launches;
+    }
+    c->split_stale = false;
     if (c->p.flags & EK_FLAG_EXPLICIT_E) {
         EK_CUDA(launch_efield_f64(c->chan, c->fields, c->stream), "efield kernel");
         ++c->launches;
     } else {
         c->e_stale = true;
     }
+    return EK_OK;
+}
+
+// Shifted storage: psif/psim from the FP64 psi plane after psi was set from
+// outside the step (fields loaded, a Poisson-Boltzmann start).
+int split_if_stale(ek_ctx *c) {
+    if (!shifted(c) || !c->split_stale) return EK_OK;
+    EK_CUDA(launch_split_psi(c->pp, c->chan, c->fields + F_PSI * c->plane, c->stream), "split psi");
+    ++c->launches;
+    c->split_stale = false;
     return EK_OK;
 }
 
@@ -464,7 +531,7 @@ int ek_create(const ek_params *p, ek_ctx **out) {
     c->plane = (size_t)p->ny * c->nxp;
     c->n = p->ny - 2;
     c->mp = round_up(p->nx / 2 + 1, 16);
-    c->keep_l2 = ek::keep_l2_fits(2 * c->plane * sizeof(double));
+    c->keep_l2 = ek::keep_l2_fits(2 * c->plane * (p->storage == EK_STORE_F64 ? sizeof(double) : sizeof(float)));
     const size_t pop_bytes = 27 * c->plane * pop_elem_bytes(p->storage);
     struct Alloc { void **ptr; size_t bytes; } allocs[] = {
         {(void **)&c->pops[0], pop_bytes},
@@ -477,9 +544,16 @@ int ek_create(const ek_params *p, ek_ctx **out) {
         {(void **)&c->pp.spec, (size_t)c->n * c->mp * sizeof(double2)},
         {(void **)&c->kref[0], 3 * (size_t)p->ny * sizeof(float)},
         {(void **)&c->kref[1], 3 * (size_t)p->ny * sizeof(float)},
+        {(void **)&c->kwall, 8 * (size_t)p->nx * sizeof(float)},
+        {(void **)&c->wdelta, 4 * (size_t)p->nx * sizeof(float)},
+        {(void **)&c->pp.rhsf, p->storage == EK_STORE_F64 ? 0 : c->plane * sizeof(float)},
+        {(void **)&c->pp.psif, p->storage == EK_STORE_F64 ? 0 : c->plane * sizeof(float)},
+        {(void **)&c->pp.psim, p->storage == EK_STORE_F64 ? 0 : (size_t)p->ny * sizeof(double)},
+        {(void **)&c->lift, p->storage == EK_STORE_F64 ? 0 : 2 * (size_t)p->nx * sizeof(float)},
         {(void **)&c->err_dev, sizeof(int)},
     };
     for (auto &a : allocs) {
+        if (a.bytes == 0) continue;
         e = cudaMalloc(a.ptr, a.bytes);
         if (e == cudaSuccess) e = cudaMemsetAsync(*a.ptr, 0, a.bytes, c->stream);
         if (e != cudaSuccess) { free_ctx(c); return cuda_fail(e, "device allocation"); }
@@ -554,6 +628,8 @@ int ek_create(const ek_params *p, ek_ctx **out) {
         if (e != cudaSuccess) { free_ctx(c); return cuda_fail(e, "FP32 Poisson set-up"); }
     }
     refresh_chan(c);
+    int rcl = upload_lift(c);
+    if (rcl != EK_OK) { free_ctx(c); return rcl; }
     *out = c;
     return EK_OK;
 }
@@ -589,6 +665,7 @@ int set_fields_from(ek_ctx *c, const double *const src[F_RHS], cudaMemcpyKind ki
         if (rc != EK_OK) return rc;
     }
     const double *ex = src[F_EX], *psi = src[F_PSI];
+    if (psi) c->split_stale = true;
     if (ex) {
         c->explicit_e_once = true;
         c->e_stale = false;
@@ -625,6 +702,13 @@ int ek_set_wall_profile(ek_ctx *c, const double *zlo, const double *zhi, const d
                 "copy wall profile");
         std::copy(src[k], src[k] + c->p.nx, c->wall_host.begin() + (size_t)k * c->p.nx);
     }
+    refresh_chan(c);  // the wall potentials' x-means
+    int rcl = upload_lift(c);
+    if (rcl != EK_OK) return rcl;
+    // shifted storage after initialisation: the wall ions' frames stay, their
+    // defect follows the new wall concentrations
+    if (shifted(c) && c->initialised)
+        EK_CUDA(launch_wall_delta(c->chan, c->kwall, c->wdelta, c->stream), "wall frames");
     EK_CUDA(cudaStreamSynchronize(c->stream), "wall profile sync");
     return EK_OK;
 }
@@ -657,6 +741,7 @@ int ek_init_poisson_boltzmann(ek_ctx *c, int32_t method, int32_t iterations, dou
         // the fields now hold E of the last Poisson solve, as the reference's do
         c->explicit_e_once = iterations > 0;
         c->e_stale = iterations == 0;
+        c->split_stale = true;
         return EK_OK;
     }
     if (method != EK_PB_NEWTON) return fail(EK_ERR_INVALID, "unknown Poisson-Boltzmann method");
@@ -697,6 +782,7 @@ int ek_init_poisson_boltzmann(ek_ctx *c, int32_t method, int32_t iterations, dou
     EK_CUDA(cudaStreamSynchronize(c->stream), "PB upload");
     c->explicit_e_once = false;
     c->e_stale = true;
+    c->split_stale = true;
     return EK_OK;
 }
 
@@ -708,7 +794,13 @@ int ek_init_equilibrium(ek_ctx *c) {
     } else {
         int rc = refs_from_fields(c, c->kref[c->kcur]);
         if (rc != EK_OK) return rc;
-        EK_CUDA(launch_init_shifted(c->chan, c->p.storage, c->pops[c->cur], c->fields, ee, c->stream), "init kernel");
+        EK_CUDA(launch_wall_frames(c->chan, c->fields, c->kq[1], c->kq[2], c->cur, c->kwall, c->wdelta, c->stream),
+                "wall frames");
+        EK_CUDA(launch_init_shifted(c->chan, c->p.storage, c->pops[c->cur], c->fields, ee, c->cur, c->stream),
+                "init kernel");
+        c->split_stale = true;  // the first step's E comes from psif/psim of the loaded psi
+        rc = split_if_stale(c);
+        if (rc != EK_OK) return rc;
     }
     // the FP32 Poisson form's row offsets start over (exact row means on the
     // first solve), so a re-initialised context repeats a fresh one bit for bit
@@ -730,6 +822,20 @@ __global__ void tile_x_planes(const T *__restrict__ src, size_t splane, int snxp
     if (x >= dnx) return;
     const size_t y = blockIdx.y, pl = blockIdx.z;
     dst[pl * dplane + y * dnxp + x] = src[pl * splane + y * snxp + x % snx];
+}
+
+// dst[r][x] = src[r][x mod snx] for rows r < rows (row pitches snx, dnx)
+template <typename T>
+__global__ void tile_x_rows(const T *__restrict__ src, int snx, T *__restrict__ dst, int dnx) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= dnx) return;
+    dst[(size_t)blockIdx.y * dnx + x] = src[(size_t)blockIdx.y * snx + x % snx];
+}
+
+template <typename T>
+cudaError_t tile_rows(const T *src, int snx, T *dst, int dnx, int rows, cudaStream_t st) {
+    tile_x_rows<T><<<dim3((dnx + 255) / 256, rows), 256, 0, st>>>(src, snx, dst, dnx);
+    return cudaGetLastError();
 }
 
 template <typename T>
@@ -760,6 +866,20 @@ int ek_tile_x(ek_ctx *dst, const ek_ctx *src) {
                                 cudaMemcpyDeviceToDevice, dst->stream),
                 "reference rows");
         for (int q = 0; q < 3; ++q) dst->kq[q] = src->kq[q];
+        // wall frames: rows of nx floats, buffer-major; the source's buffer
+        // cur becomes the destination's buffer cur
+        for (int b = 0; b < 2; ++b) {
+            const int sb = b ^ src->cur ^ dst->cur;
+            EK_CUDA(tile_rows<float>(src->kwall + (size_t)sb * 4 * src->p.nx, src->p.nx,
+                                     dst->kwall + (size_t)b * 4 * dst->p.nx, dst->p.nx, 4, dst->stream),
+                    "wall frames");
+        }
+        EK_CUDA(tile_rows<float>(src->wdelta, src->p.nx, dst->wdelta, dst->p.nx, 4, dst->stream), "wall frames");
+        // psi of the step: FP32 fluctuations tiled, row means copied
+        EK_CUDA(tile_planes<float>(src->pp.psif, src, dst->pp.psif, dst, 1, dst->stream), "psi planes");
+        EK_CUDA(cudaMemcpyAsync(dst->pp.psim, src->pp.psim, (size_t)dst->p.ny * sizeof(double),
+                                cudaMemcpyDeviceToDevice, dst->stream),
+                "psi row means");
     }
     if (dst->pp.rowmean && src->pp.rowmean) {  // offsets of the FP32 Poisson form (row means: x-independent)
         EK_CUDA(cudaMemcpyAsync(dst->pp.rowmean, src->pp.rowmean, (size_t)dst->n * sizeof(double),
@@ -774,6 +894,7 @@ int ek_tile_x(ek_ctx *dst, const ek_ctx *src) {
     dst->state_pre = src->state_pre;
     dst->explicit_e_once = src->explicit_e_once;
     dst->e_stale = src->e_stale;
+    dst->split_stale = src->split_stale;
     dst->snap_valid = false;
     refresh_chan(dst);
     return EK_OK;
@@ -783,6 +904,8 @@ int ek_step(ek_ctx *c, int32_t nsteps) {
     if (!c || nsteps < 0) return fail(EK_ERR_INVALID, "null context or negative step count");
     if (!c->initialised) return fail(EK_ERR_INVALID, "call ek_init_equilibrium before ek_step");
     const bool every = (c->p.flags & EK_FLAG_MOMENTS_EVERY_STEP) != 0;
+    int rcs = split_if_stale(c);
+    if (rcs != EK_OK) return rcs;
     for (int32_t i = 0; i < nsteps; ++i) {
         const bool ee = c->explicit_e_once || (c->p.flags & EK_FLAG_EXPLICIT_E);
         const bool rebase = shifted(c) && c->rebase_every > 0 && (c->steps + 1) % c->rebase_every == 0;
@@ -793,16 +916,16 @@ int ek_step(ek_ctx *c, int32_t nsteps) {
                                        c->fields, c->state_pre, ee, mom, c->stream);
             if (use_tma(c))
                 return launch_step_tma(c->chan, c->p.storage, &c->tmaps[c->cur], c->pops[c->cur],
-                                       c->pops[c->cur ^ 1], c->fields, c->state_pre, ee, mom, c->err_dev,
+                                       c->pops[c->cur ^ 1], c->fields, c->state_pre, ee, mom, c->cur, c->err_dev,
                                        c->wait_cycles, c->stream);
             return launch_step_shifted(c->chan, c->p.storage, c->pops[c->cur], c->pops[c->cur ^ 1], c->fields,
-                                       c->state_pre, ee, mom, c->stream);
+                                       c->state_pre, ee, mom, c->cur, c->stream);
         });
         if (rc0 != EK_OK) return rc0;
         c->cur ^= 1;
         c->state_pre = false;
         c->explicit_e_once = false;
-        int rc = poisson_now(c);
+        int rc = poisson_now(c, mom);  // the FP64 psi plane follows on the steps that write the moments
         if (rc != EK_OK) return rc;
         if (rebase) {
             rc = rebase_now(c);
@@ -827,8 +950,7 @@ int ek_set_rebase_interval(ek_ctx *c, int32_t steps) {
 
 int ek_poisson(ek_ctx *c) {
     if (!c) return fail(EK_ERR_INVALID, "null context");
-    EK_CUDA(launch_rhs_from_moments_f64(c->chan, c->fields, c->stream), "rhs kernel");
-    return poisson_now(c);
+    return poisson_now(c, true, true);
 }
 
 int ek_get_fields(ek_ctx *c, double *rho, double *ux, double *uy, double *cp, double *cn, double *psi,

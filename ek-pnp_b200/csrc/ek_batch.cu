@@ -53,7 +53,7 @@ constexpr int REFS_TPB = 256;
 template <typename S, bool FIRST, bool EE, int TXB>
 __global__ void __launch_bounds__(TXB, (EK_BATCH_SM_THREADS / TXB) > 0 ? (EK_BATCH_SM_THREADS / TXB) : 1)
 batch_lbm(const ChanF *__restrict__ chans, const S *const *__restrict__ src, S *const *__restrict__ dst,
-          double *const *__restrict__ fields, const int4 *__restrict__ tiles, int ntiles, bool mom) {
+          double *const *__restrict__ fields, const int4 *__restrict__ tiles, int ntiles, bool mom, int sbuf) {
     __shared__ ChanF ks;
     const int per = (ntiles + gridDim.x - 1) / gridDim.x;
     const int t0 = blockIdx.x * per, t1 = min(ntiles, t0 + per);
@@ -68,7 +68,7 @@ batch_lbm(const ChanF *__restrict__ chans, const S *const *__restrict__ src, S *
         }
         const int r = threadIdx.x / tl.w;
         const int x = tl.z + (threadIdx.x - r * tl.w), y = tl.y + r;
-        if (x < ks.nx && y < ks.ny) node_shifted<S, FIRST, EE>(ks, src[cur], dst[cur], fields[cur], x, y, mom);
+        if (x < ks.nx && y < ks.ny) node_shifted<S, FIRST, EE>(ks, src[cur], dst[cur], fields[cur], x, y, mom, sbuf);
     }
 }
 
@@ -112,10 +112,10 @@ __global__ void batch_commit_refs(const ChanF *__restrict__ chans, float *const 
 
 template <typename S, int TXB>
 cudaError_t lbm_t(const ChanF *chans, const void *src, void *dst, double *const *fields, const int4 *tiles,
-                  int ntiles, int grid, bool first, bool ee, bool mom, cudaStream_t s) {
+                  int ntiles, int grid, bool first, bool ee, bool mom, int sbuf, cudaStream_t s) {
     const S *const *a = (const S *const *)src;
     S *const *b = (S *const *)dst;
-#define EK_BL(F, E) batch_lbm<S, F, E, TXB><<<grid, TXB, 0, s>>>(chans, a, b, fields, tiles, ntiles, mom)
+#define EK_BL(F, E) batch_lbm<S, F, E, TXB><<<grid, TXB, 0, s>>>(chans, a, b, fields, tiles, ntiles, mom, sbuf)
     if (first) {
         if (ee) EK_BL(true, true);
         else EK_BL(true, false);
@@ -129,10 +129,10 @@ cudaError_t lbm_t(const ChanF *chans, const void *src, void *dst, double *const 
 
 template <typename S>
 cudaError_t lbm_s(int txb, const ChanF *chans, const void *src, void *dst, double *const *fields, const int4 *tiles,
-                  int ntiles, int grid, bool first, bool ee, bool mom, cudaStream_t s) {
-    if (txb == 64) return lbm_t<S, 64>(chans, src, dst, fields, tiles, ntiles, grid, first, ee, mom, s);
-    if (txb == 256) return lbm_t<S, 256>(chans, src, dst, fields, tiles, ntiles, grid, first, ee, mom, s);
-    return lbm_t<S, 128>(chans, src, dst, fields, tiles, ntiles, grid, first, ee, mom, s);
+                  int ntiles, int grid, bool first, bool ee, bool mom, int sbuf, cudaStream_t s) {
+    if (txb == 64) return lbm_t<S, 64>(chans, src, dst, fields, tiles, ntiles, grid, first, ee, mom, sbuf, s);
+    if (txb == 256) return lbm_t<S, 256>(chans, src, dst, fields, tiles, ntiles, grid, first, ee, mom, sbuf, s);
+    return lbm_t<S, 128>(chans, src, dst, fields, tiles, ntiles, grid, first, ee, mom, sbuf, s);
 }
 
 template <typename S>
@@ -285,9 +285,11 @@ int build_tables(ek_batch *b) {
     bool f32 = true;
     for (ek_ctx *c : b->ch) f32 = f32 && ek::ctx_poisson_f32(c);
     b->poisson_f32 = f32;
-    size_t field_bytes = 0;  // right-hand side + psi of the stepping channels
+    if (!f32)
+        return ek::ctx_fail(EK_ERR_UNSUPPORTED, "batched channels run the FP32 Poisson form (EK_OPT_POISSON 0 or 2)");
+    size_t field_bytes = 0;  // right-hand side + psi (FP32 planes) of the stepping channels
     for (size_t i = 0; i < b->ch.size(); ++i)
-        if (b->active[i]) field_bytes += 2 * b->ch[i]->plane * sizeof(double);
+        if (b->active[i]) field_bytes += 2 * b->ch[i]->plane * sizeof(float);
     for (ek_ctx *c : b->ch) c->keep_l2 = keep_l2_fits(field_bytes);
     for (size_t i = 0; i < b->ch.size(); ++i) {
         ek_ctx *c = b->ch[i];
@@ -309,12 +311,9 @@ int build_tables(ek_batch *b) {
             const int per = 256 / (nx >> 4);
             for (int q = 0; q < (n + 1) / 2; q += per) pairs.push_back(make_int2((int)i, q));
             const int M = poisson_tridiag_modes(n);
-            if (f32) {  // the zero mode in FP64 (modes 0..M-1 of the FP64 spectrum); modes 1.. in FP32
-                zeros.push_back(make_int3((int)i, 0, M));
-                for (int m0 = 1; m0 <= nx / 2; m0 += M) modes.push_back(make_int3((int)i, m0, M));
-            } else {
-                for (int m0 = 0; m0 <= nx / 2; m0 += M) modes.push_back(make_int3((int)i, m0, M));
-            }
+            // the zero mode in FP64 (modes 0..M-1 of the FP64 spectrum); modes 1.. in FP32
+            zeros.push_back(make_int3((int)i, 0, M));
+            for (int m0 = 1; m0 <= nx / 2; m0 += M) modes.push_back(make_int3((int)i, m0, M));
             for (int y = 0; y < c->p.ny; ++y) rows.push_back(make_int2((int)i, y));
         }
         const int nb = residual_blocks(c->chan);
@@ -356,19 +355,18 @@ int launch_step(ek_batch *b, bool first, bool ee, bool mom) {
     void *dst = b->d_pops[b->cur ^ 1];
     cudaError_t e = b->storage == EK_STORE_F16
                         ? lbm_s<__half>(b->txb, b->d_chanf, src, dst, b->d_fields, b->d_tiles, b->ntiles, b->grid,
-                                        first, ee, mom, b->stream)
+                                        first, ee, mom, b->cur, b->stream)
                         : lbm_s<float>(b->txb, b->d_chanf, src, dst, b->d_fields, b->d_tiles, b->ntiles, b->grid,
-                                       first, ee, mom, b->stream);
+                                       first, ee, mom, b->cur, b->stream);
     EK_BCUDA(e, "batch LBM kernel");
-    EK_BCUDA(batch_poisson(0, b->d_plans, b->d_chan, b->d_fields, b->d_pairs, b->npairs, b->stream, b->poisson_f32), "batch rows");
-    if (b->poisson_f32)
-        EK_BCUDA(batch_tridiag_f32_split(b->d_plans, b->d_zeros, b->nzeros, b->d_modes, b->nmodes, b->stream,
-                                         b->side, b->fork, b->join),
-                 "batch modes");
-    else
-        EK_BCUDA(batch_poisson(1, b->d_plans, b->d_chan, b->d_fields, b->d_modes, b->nmodes, b->stream, false),
-                 "batch modes");
-    EK_BCUDA(batch_poisson(2, b->d_plans, b->d_chan, b->d_fields, b->d_pairs, b->npairs, b->stream, b->poisson_f32), "batch rows");
+    EK_BCUDA(batch_poisson(0, b->d_plans, b->d_chan, b->d_fields, b->d_pairs, b->npairs, false, b->stream),
+             "batch rows");
+    EK_BCUDA(batch_tridiag_f32_split(b->d_plans, b->d_zeros, b->nzeros, b->d_modes, b->nmodes, b->stream, b->side,
+                                     b->fork, b->join),
+             "batch modes");
+    // the FP64 psi planes follow on the steps that write the moments
+    EK_BCUDA(batch_poisson(2, b->d_plans, b->d_chan, b->d_fields, b->d_pairs, b->npairs, mom, b->stream),
+             "batch rows");
     b->launches += launches_per_step(b);
     b->cur ^= 1;
     return EK_OK;

@@ -24,6 +24,7 @@ struct ek_ctx {
     bool state_pre = false;    // pops[cur] holds pre-collision populations in place
     bool explicit_e_once = false;
     bool e_stale = false;      // E planes older than psi
+    bool split_stale = false;  // shifted storage: psif/psim older than the FP64 psi plane
     double *fields = nullptr;
     double *wall = nullptr;    // 6 x nx
     std::vector<double> wall_host;  // host copy of the wall profiles
@@ -31,6 +32,9 @@ struct ek_ctx {
     double *part = nullptr;    // residual partial sums
     bool snap_valid = false;
     float *kref[2] = {nullptr, nullptr};  // shifted storage: row references /36, double-buffered
+    float *kwall = nullptr;               // shifted storage: wall ions' per-x frames (ChanF::kwall)
+    float *wdelta = nullptr;              // and half their defect (ChanF::wdelta)
+    float *lift = nullptr;                // shifted storage: the wall lifting's x-fluctuation (Chan::lift)
     int kcur = 0;
     int kq[3] = {0, 0, 0};                // binary exponents of the reference grids
     int32_t rebase_every = 0;

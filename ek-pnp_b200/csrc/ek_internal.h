@@ -60,6 +60,18 @@ __device__ __forceinline__ void st_field(double *p, double v, bool keep) {
     *p = v;
 }
 
+__device__ __forceinline__ void st_field_f(float *p, float v, bool keep) {
+#if defined(__CUDA_ARCH__)
+    if (keep) {
+        unsigned long long pol;
+        asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+        asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(p), "f"(v), "l"(pol) : "memory");
+        return;
+    }
+#endif
+    *p = v;
+}
+
 template <typename... Exp, typename... Act>
 cudaError_t launch_pdl(void (*kern)(Exp...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Act &&...args) {
     cudaLaunchConfig_t cfg = {};
@@ -111,6 +123,18 @@ struct Chan {
     // row y holds f - w_i * 36 * kref[s*ny + y]; every kref value is a
     // multiple of 2^-q, so 36 w_i (kref[y'] - kref[y]) is exact in FP32.
     const float *kref;
+    // Shifted storage only: per-x ion frames of the wall nodes (/36), per
+    // population buffer, and half their defect (see ChanF::kwall).
+    const float *kwall;
+    const float *wdelta;
+    // Shifted storage only: the step's field planes (PoissonPlan::rhsf, psif, psim),
+    // and the x-fluctuation of the wall lifting, (zeta(x) - zeta_mean)/dy^2,
+    // lower wall then upper (2 nx floats), which rows 1 and ny-2 subtract
+    // from rhsf.
+    float *rhsf;
+    const float *psif;
+    const double *psim;
+    const float *lift;
     int keep_l2;   // right-hand side and psi planes held in L2 between kernels
 };
 
@@ -131,10 +155,18 @@ cudaError_t launch_pb_conc(const Chan &c, double e_kt, double *fields, cudaStrea
 cudaError_t launch_pb_relax(const Chan &c, double omega, double *fields, double *psi_old, cudaStream_t s);
 
 // ---- shifted-storage forms (ek_lbm_f32.cu); storage = EK_STORE_F32 or _F16 ----
+// sbuf: index (0/1) of the population buffer that src is (it names the wall
+// ions' frames); buf: the buffer that pops is.
 cudaError_t launch_step_shifted(const Chan &c, int storage, const void *src, void *dst, double *fields,
-                                bool first, bool explicit_e, bool moments, cudaStream_t s);
+                                bool first, bool explicit_e, bool moments, int sbuf, cudaStream_t s);
 cudaError_t launch_init_shifted(const Chan &c, int storage, void *pops, const double *fields, bool explicit_e,
-                                cudaStream_t s);
+                                int buf, cudaStream_t s);
+// Wall frames of the ions from the fields' wall rows (initialisation; buf is
+// the buffer the initial populations go to), and their defect after the wall
+// concentrations change.
+cudaError_t launch_wall_frames(const Chan &c, const double *fields, int qp, int qn, int buf, float *kwall,
+                               float *wdelta, cudaStream_t s);
+cudaError_t launch_wall_delta(const Chan &c, const float *kwall, float *wdelta, cudaStream_t s);
 // Row means of rho, c+, c- rounded to the grid K 2^-q, stored /36 in
 // kout[3*ny] (ek_lbm_f32.cu); q per species.
 cudaError_t launch_row_refs(const Chan &c, const double *fields, int qf, int qp, int qn, float *kout,
@@ -146,7 +178,7 @@ cudaError_t launch_rebase(const Chan &c, int storage, void *pops, const float *k
 // map_out: a 128-byte CUtensorMap (64-byte aligned) over one population buffer.
 cudaError_t make_pop_tensor_map(int storage, const void *pops, int nxp, int ny, void *map_out);
 cudaError_t launch_step_tma(const Chan &c, int storage, const void *map, const void *src, void *dst, double *fields,
-                            bool first, bool explicit_e, bool moments, int *err, long long wait_cycles,
+                            bool first, bool explicit_e, bool moments, int sbuf, int *err, long long wait_cycles,
                             cudaStream_t s);
 inline size_t pop_elem_bytes(int storage) { return storage == EK_STORE_F64 ? 8 : (storage == EK_STORE_F32 ? 4 : 2); }
 
@@ -165,6 +197,18 @@ struct PoissonPlan {
     float2 *specf;              // n x mp spectrum, FP32
     double *rowmean;            // n row means of the last solve: the offset removed before the FP32 FFT
     int *rowmean_ok;            // set by the first solve's pass C; before it pass A takes exact means
+    // Field planes of the shifted-storage step (every shifted context; the
+    // FP32 form reads and writes them directly, the FP64 form through
+    // compose/split kernels):
+    //   rhsf  (ny x nxp) FP32: the right-hand side minus its row constant,
+    //         rhs_q (c+ - c- - (R+ - R-)); the constant rhs_q (R+ - R-) of the
+    //         row references and the wall lifting are added in FP64 by pass A
+    //   psif  (ny x nxp) FP32: psi minus its row mean
+    //   psim  (ny) FP64: the row means of psi (the zero mode, walls included)
+    float *rhsf;
+    float *psif;
+    double *psim;
+    double zlo_mean, zhi_mean;  // x-means of the wall potentials (psim of the wall rows)
     int keep_l2;                // psi stores ask L2 to keep the plane (see st_field)
 };
 // pass 0: row FFTs, 1: tridiagonal column solve, 2: inverse row FFTs + walls
@@ -178,22 +222,40 @@ size_t poisson_smem_bytes_f64(int nx);
 // fluctuation about each row's mean; the row sums (the zero mode), its
 // column solve and the mean of psi in FP64.
 bool poisson_f32_supported(const PoissonPlan &pp);
-// Passes 0 and 2 (pass 1 is poisson_tridiag_f32_split).
-cudaError_t poisson_pass_f32_at(int pass, const PoissonPlan &pp, const Chan &c, const double *rhs, double *psi,
-                                cudaStream_t s);
+// Passes 0 and 2 (pass 1 is poisson_tridiag_f32_split): pass 0 reads
+// pp.rhsf with the row constants of c.kref and the wall lifting; pass 2 writes
+// pp.psif and pp.psim, and the FP64 psi plane too when write_f64.
+cudaError_t poisson_pass_f32(int pass, const PoissonPlan &pp, const Chan &c, double *psi, bool write_f64,
+                             cudaStream_t s);
+// Shifted storage with the FP64 passes: the FP64 right-hand side from rhsf
+// (before pass 0), and psif/psim from the FP64 psi (after pass 2, and
+// whenever psi was set from outside).
+cudaError_t launch_compose_rhs(const PoissonPlan &pp, const Chan &c, double *rhs, cudaStream_t s);
+// The FP64 row constant of the right-hand side of row y (1 <= y <= ny-2):
+// rhs_q (R+ - R-) of the row references, minus zeta_mean/dy^2 on rows 1 and
+// ny-2 (the x-mean of the wall lifting; its fluctuation is Chan::lift).
+__host__ __device__ inline double rhs_row_constant(const PoissonPlan &pp, const Chan &c, int y) {
+    const double rq = -c.f_charge / c.eps, inv_dy2 = 1.0 / (c.dy * c.dy);
+    double v = rq * (36.0 * (double)c.kref[c.ny + y] - 36.0 * (double)c.kref[2 * c.ny + y]);
+    if (y == 1) v -= pp.zlo_mean * inv_dy2;
+    if (y == c.ny - 2) v -= pp.zhi_mean * inv_dy2;
+    return v;
+}
+cudaError_t launch_split_psi(const PoissonPlan &pp, const Chan &c, const double *psi, cudaStream_t s);
+// rhsf from the c+, c- moments (a solve outside the step, FP32 form).
+cudaError_t launch_rhsf_from_moments(const PoissonPlan &pp, const Chan &c, const double *fields, cudaStream_t s);
 // Pass B of the FP32 form as two kernels on two streams: the FP64 zero mode
 // on `side`, the FP32 modes on `s` (fork/join through the two events).
 cudaError_t poisson_tridiag_f32_split(const PoissonPlan &pp, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
                                       cudaEvent_t join);
 cudaError_t batch_tridiag_f32_split(const PoissonPlan *plans, const void *zero_items, int nzero, const void *mode_items,
                                     int nmodes, cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join);
-// Batched Poisson passes over many channels (ek_batch.cu builds the items):
-// pass 0/2 items int2 {channel, first row pair} (256-thread blocks, each
-// 256/(nx/16) row pairs; power-of-two nx from 16 to 4096); pass 1 items
-// int3 {channel, first mode, modes per block} (the FP64 form; the FP32 form's
-// pass 1 is batch_tridiag_f32_split).
+// Batched Poisson passes of the FP32 form over many channels (ek_batch.cu
+// builds the items): pass 0/2 items int2 {channel, first row pair}
+// (256-thread blocks, each 256/(nx/16) row pairs; power-of-two nx from 16 to
+// 4096); pass 1 is batch_tridiag_f32_split.  write_f64 as poisson_pass_f32.
 cudaError_t batch_poisson(int pass, const PoissonPlan *plans, const Chan *chans, double *const *fields,
-                          const void *items, int nitems, cudaStream_t s, bool f32 = false);
+                          const void *items, int nitems, bool write_f64, cudaStream_t s);
 int poisson_tridiag_modes(int n);
 // Steady-state residual sums (ek_residual.cu): per channel 8 FP64 sums,
 // (q - q_snap)^2 then q^2 for q in (ux, c+, c-, psi); the snapshot is updated.

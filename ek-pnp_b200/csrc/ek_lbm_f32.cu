@@ -35,31 +35,22 @@ ChanF make_chanf(const Chan &c) {
     k.mob_n = (float)c.mob_n;
     k.ms = (float)c.r.ms;
     k.md = (float)c.r.md;
-    k.wpd = c.r.wp;
-    k.wmd = c.r.wm;
-    k.spd = c.r.sp;
-    k.smd = c.r.sm;
-    k.kcud = 1.0 / (c.cs2 * c.cfl);
-    k.hinvcs2d = 0.5 / c.cs2;
-    k.gFd = 1.0 / (c.cfl * c.cs2);
-    k.inv_cs2d = 1.0 / c.cs2;
-    k.dtd = c.dt;
+    k.cfl_hdt = (float)(c.cfl * 0.5 * c.dt);
+    k.srcF = (float)(c.r.sm * c.cfl * c.dt);
+    k.f_chargef = (float)c.f_charge;
+    k.ext_xf = (float)c.ext_x;
+    k.exff = (float)c.exf;
+    k.half_inv_dxf = (float)(0.5 / c.dx);
+    k.half_inv_dyf = (float)(0.5 / c.dy);
+    k.rhs_qf = (float)(-c.f_charge / c.eps);
     k.f_charge = c.f_charge;
     k.eps = c.eps;
     k.ext_x = c.ext_x;
     k.exf = c.exf;
     k.dx = c.dx;
     k.dy = c.dy;
-    k.wcpd = c.r.wcp;
-    k.wcmd = c.r.wcm;
-    k.wtpd = c.r.wtp;
-    k.wtmd = c.r.wtm;
-    k.mob_pd = c.mob_p;
-    k.mob_nd = c.mob_n;
     k.half_inv_dx = 0.5 / c.dx;
     k.half_inv_dy = 0.5 / c.dy;
-    k.rhs_q = -c.f_charge / c.eps;
-    k.inv_dy2 = 1.0 / (c.dy * c.dy);
     k.zlo = c.zlo;
     k.zhi = c.zhi;
     k.cplo = c.cplo;
@@ -67,6 +58,12 @@ ChanF make_chanf(const Chan &c) {
     k.cnlo = c.cnlo;
     k.cnhi = c.cnhi;
     k.kref = c.kref;
+    k.rhsf = c.rhsf;
+    k.psif = c.psif;
+    k.psim = c.psim;
+    k.lift = c.lift;
+    k.kwall = c.kwall;
+    k.wdelta = c.wdelta;
     k.keep_l2 = c.keep_l2;
     return k;
 }
@@ -85,32 +82,45 @@ constexpr int TPB = 128;
 
 template <typename S, bool FIRST, bool EE>
 __global__ void __launch_bounds__(TPB, EK_LBM_MIN_BLOCKS)
-step_shifted(const ChanF k, const S *__restrict__ src, S *__restrict__ dst, double *__restrict__ fields, bool mom) {
+step_shifted(const ChanF k, const S *__restrict__ src, S *__restrict__ dst, double *__restrict__ fields, bool mom,
+             int sbuf) {
     const int x = blockIdx.x * TPB + threadIdx.x;
     if (x >= k.nx) return;
-    node_shifted<S, FIRST, EE>(k, src, dst, fields, x, blockIdx.y, mom);
+    node_shifted<S, FIRST, EE>(k, src, dst, fields, x, blockIdx.y, mom, sbuf);
 }
 
 template <typename S>
 __global__ void __launch_bounds__(TPB)
-init_shifted(const ChanF k, S *__restrict__ pops, const double *__restrict__ fields, bool explicit_e) {
+init_shifted(const ChanF k, S *__restrict__ pops, const double *__restrict__ fields, bool explicit_e, int buf) {
     const int x = blockIdx.x * TPB + threadIdx.x;
     if (x >= k.nx) return;
-    init_node_shifted<S>(k, pops, fields, explicit_e, x, blockIdx.y);
+    init_node_shifted<S>(k, pops, fields, explicit_e, x, blockIdx.y, buf);
+}
+
+__global__ void __launch_bounds__(256) wall_frames(const ChanF k, const double *__restrict__ fields, int qp, int qn,
+                                                   int buf, float *__restrict__ kwall, float *__restrict__ wdelta) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < 4 * k.nx) wall_frames_dev(k, fields, qp, qn, buf, kwall, wdelta, i);
+}
+
+__global__ void __launch_bounds__(256) wall_delta(const ChanF k, const float *__restrict__ kwall,
+                                                  float *__restrict__ wdelta) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < 4 * k.nx) wall_delta_dev(k, kwall, wdelta, i);
 }
 
 template <typename S>
 cudaError_t step_typed(const ChanF &k, const void *src, void *dst, double *fields, bool first, bool ee,
-                       bool mom, cudaStream_t s) {
+                       bool mom, int sbuf, cudaStream_t s) {
     const dim3 g((k.nx + TPB - 1) / TPB, k.ny);
     const S *a = (const S *)src;
     S *b = (S *)dst;
     if (first) {
-        if (ee) step_shifted<S, true, true><<<g, TPB, 0, s>>>(k, a, b, fields, mom);
-        else step_shifted<S, true, false><<<g, TPB, 0, s>>>(k, a, b, fields, mom);
+        if (ee) step_shifted<S, true, true><<<g, TPB, 0, s>>>(k, a, b, fields, mom, sbuf);
+        else step_shifted<S, true, false><<<g, TPB, 0, s>>>(k, a, b, fields, mom, sbuf);
     } else {
-        if (ee) step_shifted<S, false, true><<<g, TPB, 0, s>>>(k, a, b, fields, mom);
-        else step_shifted<S, false, false><<<g, TPB, 0, s>>>(k, a, b, fields, mom);
+        if (ee) step_shifted<S, false, true><<<g, TPB, 0, s>>>(k, a, b, fields, mom, sbuf);
+        else step_shifted<S, false, false><<<g, TPB, 0, s>>>(k, a, b, fields, mom, sbuf);
     }
     return cudaGetLastError();
 }
@@ -129,7 +139,69 @@ __global__ void __launch_bounds__(TPB) rebase_pops(const Chan c, S *__restrict__
     rebase_dev<S>(pops + (size_t)plane * c.plane + (size_t)y * c.nxp + x, plane, c.ny, y, kold, knew);
 }
 
+// psim[y] = the row's FP64 mean of psi, psif = psi - psim in FP32; a block
+// of 256 threads per row.
+__global__ void __launch_bounds__(256) split_psi(const PoissonPlan pp, const Chan c, const double *__restrict__ psi) {
+    const int y = blockIdx.x;
+    const double *r = psi + (size_t)y * c.nxp;
+    double acc = 0.0;
+    for (int x = threadIdx.x; x < c.nx; x += 256) acc += r[x];
+    __shared__ double red[8];
+    __shared__ double mean;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = 0.0;
+        for (int w = 0; w < 8; ++w) v += red[w];
+        mean = v / (double)c.nx;
+        pp.psim[y] = mean;
+    }
+    __syncthreads();
+    float *f = pp.psif + (size_t)y * c.nxp;
+    for (int x = threadIdx.x; x < c.nx; x += 256) f[x] = (float)(r[x] - mean);
+}
+
+// The FP64 right-hand side of the interior rows from rhsf: the row constant
+// rhs_q (R+ - R-) and the wall lifting added back (the FP64 passes' input).
+__global__ void __launch_bounds__(TPB) compose_rhs(const PoissonPlan pp, const Chan c, double *__restrict__ rhs) {
+    const int x = blockIdx.x * TPB + threadIdx.x, y = blockIdx.y + 1;
+    if (x >= c.nx) return;
+    const size_t o = (size_t)y * c.nxp + x;
+    rhs[o] = (double)pp.rhsf[o] + rhs_row_constant(pp, c, y);
+}
+
+// rhsf of the interior rows from the c+, c- moments (a solve outside the step).
+__global__ void __launch_bounds__(TPB) rhsf_from_moments(const PoissonPlan pp, const Chan c,
+                                                         const double *__restrict__ fields) {
+    const int x = blockIdx.x * TPB + threadIdx.x, y = blockIdx.y + 1;
+    if (x >= c.nx) return;
+    const size_t o = (size_t)y * c.nxp + x;
+    const double rq = -c.f_charge / c.eps;
+    const double q = fields[F_CP * c.plane + o] - fields[F_CN * c.plane + o];
+    double v = rq * (q - (36.0 * (double)c.kref[c.ny + y] - 36.0 * (double)c.kref[2 * c.ny + y]));
+    if (y == 1) v -= c.lift[x];
+    if (y == c.ny - 2) v -= c.lift[c.nx + x];
+    pp.rhsf[o] = (float)v;
+}
+
 }  // namespace
+
+cudaError_t launch_split_psi(const PoissonPlan &pp, const Chan &c, const double *psi, cudaStream_t s) {
+    split_psi<<<c.ny, 256, 0, s>>>(pp, c, psi);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_compose_rhs(const PoissonPlan &pp, const Chan &c, double *rhs, cudaStream_t s) {
+    compose_rhs<<<dim3((c.nx + TPB - 1) / TPB, c.ny - 2), TPB, 0, s>>>(pp, c, rhs);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rhsf_from_moments(const PoissonPlan &pp, const Chan &c, const double *fields, cudaStream_t s) {
+    rhsf_from_moments<<<dim3((c.nx + TPB - 1) / TPB, c.ny - 2), TPB, 0, s>>>(pp, c, fields);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_row_refs(const Chan &c, const double *fields, int qf, int qp, int qn, float *kout,
                             cudaStream_t s) {
@@ -146,18 +218,31 @@ cudaError_t launch_rebase(const Chan &c, int storage, void *pops, const float *k
 }
 
 cudaError_t launch_step_shifted(const Chan &c, int storage, const void *src, void *dst, double *fields,
-                                bool first, bool explicit_e, bool moments, cudaStream_t s) {
+                                bool first, bool explicit_e, bool moments, int sbuf, cudaStream_t s) {
     const ChanF k = make_chanf(c);
-    if (storage == EK_STORE_F16) return step_typed<__half>(k, src, dst, fields, first, explicit_e, moments, s);
-    return step_typed<float>(k, src, dst, fields, first, explicit_e, moments, s);
+    if (storage == EK_STORE_F16) return step_typed<__half>(k, src, dst, fields, first, explicit_e, moments, sbuf, s);
+    return step_typed<float>(k, src, dst, fields, first, explicit_e, moments, sbuf, s);
 }
 
 cudaError_t launch_init_shifted(const Chan &c, int storage, void *pops, const double *fields, bool explicit_e,
-                                cudaStream_t s) {
+                                int buf, cudaStream_t s) {
     const ChanF k = make_chanf(c);
     const dim3 g((k.nx + TPB - 1) / TPB, k.ny);
-    if (storage == EK_STORE_F16) init_shifted<__half><<<g, TPB, 0, s>>>(k, (__half *)pops, fields, explicit_e);
-    else init_shifted<float><<<g, TPB, 0, s>>>(k, (float *)pops, fields, explicit_e);
+    if (storage == EK_STORE_F16) init_shifted<__half><<<g, TPB, 0, s>>>(k, (__half *)pops, fields, explicit_e, buf);
+    else init_shifted<float><<<g, TPB, 0, s>>>(k, (float *)pops, fields, explicit_e, buf);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wall_frames(const Chan &c, const double *fields, int qp, int qn, int buf, float *kwall,
+                               float *wdelta, cudaStream_t s) {
+    const ChanF k = make_chanf(c);
+    wall_frames<<<(4 * c.nx + 255) / 256, 256, 0, s>>>(k, fields, qp, qn, buf, kwall, wdelta);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wall_delta(const Chan &c, const float *kwall, float *wdelta, cudaStream_t s) {
+    const ChanF k = make_chanf(c);
+    wall_delta<<<(4 * c.nx + 255) / 256, 256, 0, s>>>(k, kwall, wdelta);
     return cudaGetLastError();
 }
 

@@ -98,7 +98,7 @@ template <> __device__ __forceinline__ float ld_smem<__half>(const __half *p) { 
 template <typename S, bool FIRST, bool EE>
 __global__ void __launch_bounds__(NTHREADS)
 step_tma(const __grid_constant__ CUtensorMap tsrc, const ChanF k, const S *__restrict__ src, S *__restrict__ dst,
-         double *__restrict__ fields, int *__restrict__ err, bool mom, long long wait_cycles) {
+         double *__restrict__ fields, int *__restrict__ err, bool mom, long long wait_cycles, int sbuf) {
     using G = Geom<S>;
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *full = (uint64_t *)(smem + NSTAGE * G::STAGE_BYTES);
@@ -175,7 +175,7 @@ step_tma(const __grid_constant__ CUtensorMap tsrc, const ChanF k, const S *__res
                     v[plane] = ld_pop<S>(src + plane * pl + (size_t)row * k.nxp + xs);
                 }
             }
-            collide_shifted<S, FIRST, EE>(k, v, v + 9, v + 18, src, dst, fields, x, y, mom);
+            collide_shifted<S, FIRST, EE>(k, v, v + 9, v + 18, src, dst, fields, x, y, mom, sbuf);
         }
     }
 }
@@ -194,12 +194,13 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 template <typename S>
 cudaError_t launch_typed(const CUtensorMap &map, const ChanF &k, const void *src, void *dst, double *fields,
-                         bool first, bool ee, bool mom, int *err, long long wait_cycles, int grid,
+                         bool first, bool ee, bool mom, int sbuf, int *err, long long wait_cycles, int grid,
                          cudaStream_t s) {
     const S *a = (const S *)src;
     S *b = (S *)dst;
     const int smem = Geom<S>::SMEM_BYTES;
-#define EK_TMA(F, E) step_tma<S, F, E><<<grid, NTHREADS, smem, s>>>(map, k, a, b, fields, err, mom, wait_cycles)
+#define EK_TMA(F, E) \
+    step_tma<S, F, E><<<grid, NTHREADS, smem, s>>>(map, k, a, b, fields, err, mom, wait_cycles, sbuf)
     if (first) {
         if (ee) EK_TMA(true, true);
         else EK_TMA(true, false);
@@ -241,7 +242,7 @@ cudaError_t make_pop_tensor_map(int storage, const void *pops, int nxp, int ny, 
 }
 
 cudaError_t launch_step_tma(const Chan &c, int storage, const void *map, const void *src, void *dst, double *fields,
-                            bool first, bool explicit_e, bool moments, int *err, long long wait_cycles,
+                            bool first, bool explicit_e, bool moments, int sbuf, int *err, long long wait_cycles,
                             cudaStream_t s) {
     static bool attrs = false;
     if (!attrs) {
@@ -264,8 +265,10 @@ cudaError_t launch_step_tma(const Chan &c, int storage, const void *map, const v
     int grid = sms * (per > 0 ? per : 1);
     if (grid > ntiles) grid = ntiles;
     const CUtensorMap &m = *(const CUtensorMap *)map;
-    return half ? launch_typed<__half>(m, k, src, dst, fields, first, explicit_e, moments, err, wait_cycles, grid, s)
-                : launch_typed<float>(m, k, src, dst, fields, first, explicit_e, moments, err, wait_cycles, grid, s);
+    return half ? launch_typed<__half>(m, k, src, dst, fields, first, explicit_e, moments, sbuf, err, wait_cycles,
+                                       grid, s)
+                : launch_typed<float>(m, k, src, dst, fields, first, explicit_e, moments, sbuf, err, wait_cycles,
+                                      grid, s);
 }
 
 }  // namespace ek

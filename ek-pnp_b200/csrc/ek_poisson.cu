@@ -407,12 +407,16 @@ __device__ __forceinline__ double group_sum(double v, int T, double *red) {
 // Pass A of the FP32 form for 2^K-point rows: the FP64 row sums (the zero
 // mode) and the FP32 transform of the fluctuation about an offset (it only
 // moves the unused FP32 zero bin; a close one keeps the rounding small).
+// A row's right-hand side is rhsf plus, in FP64, the row constant: rhs_q
+// (R+ - R-) of the row references and, on rows 1 and ny-2, the x-mean of the
+// Dirichlet lifting -zeta/dy^2 (odd_extension, poisson.cu:228-241; its
+// x-fluctuation is in rhsf).
 // From the second solve on the offset is the previous solve's row mean and
 // one pass over the row does both; the first solve takes two passes and the
 // exact mean.  The first radix-16 pass runs on the values as loaded.
 template <int BLOCK, int K>
-__device__ __forceinline__ void fwd_rows_f32_k(const PoissonPlan &pp, const double *__restrict__ rhs, int nxp,
-                                               int pair_base, float2 *sm, double *red) {
+__device__ __forceinline__ void fwd_rows_f32_k(const PoissonPlan &pp, const Chan &c, int pair_base, float2 *sm,
+                                               double *red) {
     using S = fft32::Shape<K>;
     constexpr int N = S::N, T = S::T;
     const int p = threadIdx.x / T, t = threadIdx.x - p * T;
@@ -420,27 +424,30 @@ __device__ __forceinline__ void fwd_rows_f32_k(const PoissonPlan &pp, const doub
     float2 *s = sm + p * N;
     const int j0 = 2 * pair, j1 = j0 + 1;
     const bool live = j0 < pp.n, two = j1 < pp.n;
-    const double *r0 = rhs + (size_t)(j0 + 1) * nxp + t, *r1 = rhs + (size_t)(j1 + 1) * nxp + t;
+    const int nxp = c.nxp;
+    const float *r0 = pp.rhsf + (size_t)(j0 + 1) * nxp + t, *r1 = pp.rhsf + (size_t)(j1 + 1) * nxp + t;
+    const double k0 = live ? rhs_row_constant(pp, c, j0 + 1) : 0.0, k1 = two ? rhs_row_constant(pp, c, j1 + 1) : 0.0;
     const bool exact = *pp.rowmean_ok == 0;  // the same for every block of the launch
-    double e0 = (live && !exact) ? pp.rowmean[j0] : 0.0, e1 = (two && !exact) ? pp.rowmean[j1] : 0.0;
+    // value - offset = rhsf + (row constant - offset)
+    double d0 = (live && !exact) ? k0 - pp.rowmean[j0] : 0.0, d1 = (two && !exact) ? k1 - pp.rowmean[j1] : 0.0;
     double a0 = 0.0, a1 = 0.0;
     float2 x[16];
 #pragma unroll
     for (int v = 0; v < 16; ++v) {
-        const double v0 = live ? __ldg(r0 + v * T) : 0.0, v1 = two ? __ldg(r1 + v * T) : 0.0;
-        a0 += v0;
-        a1 += v1;
-        x[v] = make_float2((float)(v0 - e0), (float)(v1 - e1));
+        const float f0 = live ? __ldg(r0 + v * T) : 0.0f, f1 = two ? __ldg(r1 + v * T) : 0.0f;
+        a0 += (double)f0;
+        a1 += (double)f1;
+        x[v] = make_float2((float)((double)f0 + d0), (float)((double)f1 + d1));
     }
-    a0 = group_sum<BLOCK>(a0, T, red);
-    a1 = group_sum<BLOCK>(a1, T, red);
+    a0 = group_sum<BLOCK>(a0, T, red) + (double)N * k0;
+    a1 = group_sum<BLOCK>(a1, T, red) + (double)N * k1;
     if (exact) {
-        e0 = a0 / (double)N;
-        e1 = a1 / (double)N;
+        d0 = k0 - a0 / (double)N;
+        d1 = k1 - a1 / (double)N;
 #pragma unroll
         for (int v = 0; v < 16; ++v)
-            x[v] = make_float2(live ? (float)(__ldg(r0 + v * T) - e0) : 0.0f,
-                               two ? (float)(__ldg(r1 + v * T) - e1) : 0.0f);
+            x[v] = make_float2(live ? (float)((double)__ldg(r0 + v * T) + d0) : 0.0f,
+                               two ? (float)((double)__ldg(r1 + v * T) + d1) : 0.0f);
     }
     if (t == 0 && live) {
         pp.spec[(size_t)j0 * pp.mp] = make_double2(a0, 0.0);
@@ -463,13 +470,34 @@ __device__ __forceinline__ void fwd_rows_f32_k(const PoissonPlan &pp, const doub
     }
 }
 
+// Wall rows of the FP32 form's psi: psim = the x-mean of the wall potential,
+// psif = the potential minus it (zero for uniform walls), the FP64 plane's
+// Dirichlet values too when write_f64; spread over the nb blocks of the pass.
+__device__ __forceinline__ void write_walls_f32(const PoissonPlan &pp, const Chan &c, double *__restrict__ psi,
+                                                bool write_f64, int lb, int nb, int bs) {
+    const int nx = c.nx, ny = c.ny;
+    float *flo = pp.psif, *fhi = pp.psif + (size_t)(ny - 1) * c.nxp;
+    double *dlo = psi, *dhi = psi + (size_t)(ny - 1) * c.nxp;
+    for (int g = lb * bs + (int)threadIdx.x; g < 2 * nx; g += nb * bs) {
+        const bool low = g < nx;
+        const int x = low ? g : g - nx;
+        const double z = __ldg((low ? c.zlo : c.zhi) + x);
+        (low ? flo : fhi)[x] = (float)(z - (low ? pp.zlo_mean : pp.zhi_mean));
+        if (write_f64) (low ? dlo : dhi)[x] = z;
+    }
+    if (lb == 0 && threadIdx.x == 0) {
+        pp.psim[0] = pp.zlo_mean;
+        pp.psim[ny - 1] = pp.zhi_mean;
+    }
+}
+
 // Pass C of the FP32 form: the two real rows' spectra packed as A + iB, the
-// inverse transform, psi = FP64 row mean + FP32 fluctuation / N; the last
-// radix-16 pass writes psi from registers.
+// inverse transform; psif = the FP32 fluctuation / N (stored from registers by
+// the last radix-16 pass), psim = the FP64 row mean, and the FP64 psi plane
+// (mean + fluctuation) when write_f64.
 template <int BLOCK, int K>
-__device__ __forceinline__ void inv_rows_f32_k(const PoissonPlan &pp, int nxp, int ny, const double *zlo,
-                                               const double *zhi, double *__restrict__ psi, int pair_base,
-                                               float2 *sm) {
+__device__ __forceinline__ void inv_rows_f32_k(const PoissonPlan &pp, const Chan &c, double *__restrict__ psi,
+                                               bool write_f64, int pair_base, float2 *sm) {
     using S = fft32::Shape<K>;
     constexpr int N = S::N, T = S::T;
     const int p = threadIdx.x / T, t = threadIdx.x - p * T;
@@ -477,8 +505,9 @@ __device__ __forceinline__ void inv_rows_f32_k(const PoissonPlan &pp, int nxp, i
     float2 *s = sm + p * N;
     const int j0 = 2 * pair, j1 = j0 + 1;
     const bool live = j0 < pp.n, two = j1 < pp.n;
+    const int nxp = c.nxp;
     constexpr int per = BLOCK / T;
-    write_walls(psi, zlo, zhi, N, ny, nxp, pair_base / per, ((pp.n + 1) / 2 + per - 1) / per, BLOCK);
+    write_walls_f32(pp, c, psi, write_f64, pair_base / per, ((pp.n + 1) / 2 + per - 1) / per, BLOCK);
     const float2 *s0 = pp.specf + (size_t)j0 * pp.mp, *s1 = pp.specf + (size_t)j1 * pp.mp;
     // modes m = t + i T (i < 8) and, for t = 0, m = N/2: all loads first
     const float2 zero = make_float2(0.0f, 0.0f);
@@ -504,15 +533,26 @@ __device__ __forceinline__ void inv_rows_f32_k(const PoissonPlan &pp, int nxp, i
     float2 x[16];
     fft32::inv_pass_load<K, 1>(x, s, t, p, pp.twf);
     const double inv = 1.0 / (double)N;
+    const float invf = 1.0f / (float)N;  // a power of two: exact
     if (pair_base == 0 && threadIdx.x == 0) *pp.rowmean_ok = 1;
     if (live) {
         const double mean0 = pp.spec[(size_t)j0 * pp.mp].x * inv;
         const double mean1 = two ? pp.spec[(size_t)j1 * pp.mp].x * inv : 0.0;
+        if (t == 0) {
+            pp.psim[j0 + 1] = mean0;
+            if (two) pp.psim[j1 + 1] = mean1;
+        }
+        float *f0 = pp.psif + (size_t)(j0 + 1) * nxp + t, *f1 = pp.psif + (size_t)(j1 + 1) * nxp + t;
         double *p0 = psi + (size_t)(j0 + 1) * nxp + t, *p1 = psi + (size_t)(j1 + 1) * nxp + t;
 #pragma unroll
         for (int v = 0; v < 16; ++v) {
-            st_field(p0 + v * T, mean0 + (double)x[v].x * inv, pp.keep_l2);
-            if (two) st_field(p1 + v * T, mean1 + (double)x[v].y * inv, pp.keep_l2);
+            const float q0 = x[v].x * invf, q1 = x[v].y * invf;
+            st_field_f(f0 + v * T, q0, pp.keep_l2);
+            if (two) st_field_f(f1 + v * T, q1, pp.keep_l2);
+            if (write_f64) {
+                p0[v * T] = mean0 + (double)q0;
+                if (two) p1[v * T] = mean1 + (double)q1;
+            }
         }
     }
 }
@@ -527,12 +567,12 @@ template <int BLOCK, int K> __host__ __device__ constexpr bool r16f_fits() {
 #define EK_R16F_CASES(F) F(4) F(5) F(6) F(7) F(8) F(9) F(10) F(11) F(12) F(13)
 
 template <int BLOCK>
-__device__ __forceinline__ void fwd_rows_r16f_dev(const PoissonPlan &pp, const double *__restrict__ rhs, int nxp,
-                                                  int pair_base, float2 *sm, double *red) {
+__device__ __forceinline__ void fwd_rows_r16f_dev(const PoissonPlan &pp, const Chan &c, int pair_base, float2 *sm,
+                                                  double *red) {
     switch (pp.log2nx) {
 #define EK_CASE(K)                                                                        \
     case K:                                                                               \
-        if constexpr (r16f_fits<BLOCK, K>()) fwd_rows_f32_k<BLOCK, K>(pp, rhs, nxp, pair_base, sm, red); \
+        if constexpr (r16f_fits<BLOCK, K>()) fwd_rows_f32_k<BLOCK, K>(pp, c, pair_base, sm, red); \
         break;
         EK_R16F_CASES(EK_CASE)
 #undef EK_CASE
@@ -541,13 +581,12 @@ __device__ __forceinline__ void fwd_rows_r16f_dev(const PoissonPlan &pp, const d
 }
 
 template <int BLOCK>
-__device__ __forceinline__ void inv_rows_r16f_dev(const PoissonPlan &pp, int nxp, int ny, const double *zlo,
-                                                  const double *zhi, double *__restrict__ psi, int pair_base,
-                                                  float2 *sm) {
+__device__ __forceinline__ void inv_rows_r16f_dev(const PoissonPlan &pp, const Chan &c, double *__restrict__ psi,
+                                                  bool write_f64, int pair_base, float2 *sm) {
     switch (pp.log2nx) {
 #define EK_CASE(K)                                                                                    \
     case K:                                                                                           \
-        if constexpr (r16f_fits<BLOCK, K>()) inv_rows_f32_k<BLOCK, K>(pp, nxp, ny, zlo, zhi, psi, pair_base, sm); \
+        if constexpr (r16f_fits<BLOCK, K>()) inv_rows_f32_k<BLOCK, K>(pp, c, psi, write_f64, pair_base, sm); \
         break;
         EK_R16F_CASES(EK_CASE)
 #undef EK_CASE
@@ -559,19 +598,18 @@ __device__ __forceinline__ void inv_rows_r16f_dev(const PoissonPlan &pp, int nxp
 // then run in one wave (3 blocks per SM leave a second, nearly empty wave).
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
-fwd_rows_r16f(const PoissonPlan pp, const double *__restrict__ rhs, int nxp) {
+fwd_rows_r16f(const PoissonPlan pp, const Chan c) {
     pdl_wait();
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ double red[BLOCK / 32];
-    fwd_rows_r16f_dev<BLOCK>(pp, rhs, nxp, blockIdx.x * (BLOCK / (pp.nx >> 4)), (float2 *)smraw, red);
+    fwd_rows_r16f_dev<BLOCK>(pp, c, blockIdx.x * (BLOCK / (pp.nx >> 4)), (float2 *)smraw, red);
 }
 
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
-inv_rows_r16f(const PoissonPlan pp, const Chan c, double *__restrict__ psi) {
+inv_rows_r16f(const PoissonPlan pp, const Chan c, double *__restrict__ psi, bool write_f64) {
     extern __shared__ __align__(16) unsigned char smraw[];
-    inv_rows_r16f_dev<BLOCK>(pp, c.nxp, c.ny, c.zlo, c.zhi, psi, blockIdx.x * (BLOCK / (pp.nx >> 4)),
-                             (float2 *)smraw);
+    inv_rows_r16f_dev<BLOCK>(pp, c, psi, write_f64, blockIdx.x * (BLOCK / (pp.nx >> 4)), (float2 *)smraw);
 }
 
 // ---- pass B, partitioned Thomas solve ------------------------------------
@@ -713,26 +751,7 @@ __global__ void __launch_bounds__(TB_THREADS, 2) tridiag_modes_f32(const Poisson
 // ---- batched passes: one launch for many channels -------------------------
 // A block's work item names its channel and its first row pair (passes A,
 // C) or first x-mode (pass B); the channel's plan comes from a device table.
-__global__ void __launch_bounds__(256, 2)
-batch_fwd_rows(const PoissonPlan *__restrict__ plans, const Chan *__restrict__ chans,
-               double *const *__restrict__ fields, const int2 *__restrict__ items) {
-    extern __shared__ double2 sm[];
-    const int2 it = items[blockIdx.x];
-    const PoissonPlan pp = plans[it.x];
-    const Chan &c = chans[it.x];
-    fwd_rows_r16_dev<256>(pp, fields[it.x] + F_RHS * c.plane, c.nxp, it.y, sm);
-}
-
-__global__ void __launch_bounds__(256, 2)
-batch_inv_rows(const PoissonPlan *__restrict__ plans, const Chan *__restrict__ chans,
-               double *const *__restrict__ fields, const int2 *__restrict__ items) {
-    extern __shared__ double2 sm[];
-    const int2 it = items[blockIdx.x];
-    const PoissonPlan pp = plans[it.x];
-    const Chan &c = chans[it.x];
-    inv_rows_r16_dev<256>(pp, c.nxp, c.ny, c.zlo, c.zhi, fields[it.x] + F_PSI * c.plane, it.y, sm);
-}
-
+// Batches run the FP32 form; the zero modes' FP64 column solve is batch_tridiag.
 __global__ void __launch_bounds__(TB_THREADS)
 batch_tridiag(const PoissonPlan *__restrict__ plans, const int3 *__restrict__ items) {
     __shared__ TridiagShared sh;
@@ -743,23 +762,22 @@ batch_tridiag(const PoissonPlan *__restrict__ plans, const int3 *__restrict__ it
 
 __global__ void __launch_bounds__(256, 4)
 batch_fwd_rows_f32(const PoissonPlan *__restrict__ plans, const Chan *__restrict__ chans,
-                   double *const *__restrict__ fields, const int2 *__restrict__ items) {
+                   const int2 *__restrict__ items) {
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ double red[256 / 32];
     const int2 it = items[blockIdx.x];
     const PoissonPlan pp = plans[it.x];
-    const Chan &c = chans[it.x];
-    fwd_rows_r16f_dev<256>(pp, fields[it.x] + F_RHS * c.plane, c.nxp, it.y, (float2 *)smraw, red);
+    fwd_rows_r16f_dev<256>(pp, chans[it.x], it.y, (float2 *)smraw, red);
 }
 
 __global__ void __launch_bounds__(256, 4)
 batch_inv_rows_f32(const PoissonPlan *__restrict__ plans, const Chan *__restrict__ chans,
-                   double *const *__restrict__ fields, const int2 *__restrict__ items) {
+                   double *const *__restrict__ fields, const int2 *__restrict__ items, bool write_f64) {
     extern __shared__ __align__(16) unsigned char smraw[];
     const int2 it = items[blockIdx.x];
     const PoissonPlan pp = plans[it.x];
     const Chan &c = chans[it.x];
-    inv_rows_r16f_dev<256>(pp, c.nxp, c.ny, c.zlo, c.zhi, fields[it.x] + F_PSI * c.plane, it.y, (float2 *)smraw);
+    inv_rows_r16f_dev<256>(pp, c, fields[it.x] + F_PSI * c.plane, write_f64, it.y, (float2 *)smraw);
 }
 
 // items {channel, first mode, modes per block}: FP32 mode blocks (the zero
@@ -852,8 +870,8 @@ cudaError_t poisson_tridiag_f32_split(const PoissonPlan &pp, cudaStream_t s, cud
     return e;
 }
 
-cudaError_t poisson_pass_f32_at(int pass, const PoissonPlan &pp, const Chan &c, const double *rhs, double *psi,
-                                cudaStream_t s) {
+cudaError_t poisson_pass_f32(int pass, const PoissonPlan &pp, const Chan &c, double *psi, bool write_f64,
+                             cudaStream_t s) {
     // pass B of this form runs through poisson_tridiag_f32_split
     if (!poisson_f32_supported(pp) || pass == 1) return cudaErrorInvalidValue;
     int threads, per;
@@ -861,32 +879,23 @@ cudaError_t poisson_pass_f32_at(int pass, const PoissonPlan &pp, const Chan &c, 
     const size_t smem = (size_t)per * pp.nx * sizeof(float2);
     const int blocks = ((pp.n + 1) / 2 + per - 1) / per;
     if (threads == 256) {
-        if (pass == 0) return launch_pdl(fwd_rows_r16f<256>, dim3(blocks), dim3(256), smem, s, pp, rhs, c.nxp);
-        inv_rows_r16f<256><<<blocks, 256, smem, s>>>(pp, c, psi);
+        if (pass == 0) return launch_pdl(fwd_rows_r16f<256>, dim3(blocks), dim3(256), smem, s, pp, c);
+        inv_rows_r16f<256><<<blocks, 256, smem, s>>>(pp, c, psi, write_f64);
     } else {
-        if (pass == 0) return launch_pdl(fwd_rows_r16f<512>, dim3(blocks), dim3(512), smem, s, pp, rhs, c.nxp);
-        inv_rows_r16f<512><<<blocks, 512, smem, s>>>(pp, c, psi);
+        if (pass == 0) return launch_pdl(fwd_rows_r16f<512>, dim3(blocks), dim3(512), smem, s, pp, c);
+        inv_rows_r16f<512><<<blocks, 512, smem, s>>>(pp, c, psi, write_f64);
     }
     return cudaGetLastError();
 }
 
 cudaError_t batch_poisson(int pass, const PoissonPlan *plans, const Chan *chans, double *const *fields,
-                          const void *items, int nitems, cudaStream_t s, bool f32) {
+                          const void *items, int nitems, bool write_f64, cudaStream_t s) {
     if (nitems <= 0) return cudaSuccess;
-    if (f32) {
-        if (pass == 1) return cudaErrorInvalidValue;  // runs through batch_tridiag_f32_split
-        if (pass == 0)
-            batch_fwd_rows_f32<<<nitems, 256, 32768, s>>>(plans, chans, fields, (const int2 *)items);
-        else
-            batch_inv_rows_f32<<<nitems, 256, 32768, s>>>(plans, chans, fields, (const int2 *)items);
-        return cudaGetLastError();
-    }
+    if (pass == 1) return cudaErrorInvalidValue;  // runs through batch_tridiag_f32_split
     if (pass == 0)
-        batch_fwd_rows<<<nitems, 256, 65536, s>>>(plans, chans, fields, (const int2 *)items);
-    else if (pass == 1)
-        batch_tridiag<<<nitems, TB_THREADS, 0, s>>>(plans, (const int3 *)items);
+        batch_fwd_rows_f32<<<nitems, 256, 32768, s>>>(plans, chans, (const int2 *)items);
     else
-        batch_inv_rows<<<nitems, 256, 65536, s>>>(plans, chans, fields, (const int2 *)items);
+        batch_inv_rows_f32<<<nitems, 256, 32768, s>>>(plans, chans, fields, (const int2 *)items, write_f64);
     return cudaGetLastError();
 }
 
@@ -906,8 +915,7 @@ cudaError_t batch_tridiag_f32_split(const PoissonPlan *plans, const void *zero_i
 cudaError_t poisson_set_smem_limits() {
     const void *fns[] = {(const void *)fwd_rows, (const void *)inv_rows, (const void *)fwd_rows_r16<256>,
                          (const void *)inv_rows_r16<256>, (const void *)fwd_rows_r16<512>,
-                         (const void *)inv_rows_r16<512>, (const void *)batch_fwd_rows,
-                         (const void *)batch_inv_rows, (const void *)fwd_rows_r16f<256>,
+                         (const void *)inv_rows_r16<512>, (const void *)fwd_rows_r16f<256>,
                          (const void *)inv_rows_r16f<256>, (const void *)fwd_rows_r16f<512>,
                          (const void *)inv_rows_r16f<512>, (const void *)batch_fwd_rows_f32,
                          (const void *)batch_inv_rows_f32};

@@ -350,7 +350,8 @@ def xreduced_start_run(specs, start="cold", surrogate=None, narrow_nx=16, tol=1e
     make the steady state independent of x, so each channel first relaxes on
     narrow_nx columns (start "cold": the uniform cold start; "surrogate": the
     network's start, judged as in warm_start_run with the cold start as
-    fallback), then its relaxed state is tiled along x into the full channel
+    fallback; "physics": the Poisson-Boltzmann/electro-osmotic start without
+    the network), then its relaxed state is tiled along x into the full channel
     (ek_tile_x) and the full batch steps to the same residual.  Steps and wall
     time count both stages (inference, both batches' set-up and the copies
     included).  narrow_max_steps caps the narrow stage (default max_steps):
@@ -365,8 +366,11 @@ def xreduced_start_run(specs, start="cold", surrogate=None, narrow_nx=16, tol=1e
     elif start == "cold":
         nfields = [cold_state(s) for s in nspecs]
         judge = None
+    elif start == "physics":
+        nfields = [profile_fields(s, physics_profiles(s)) for s in nspecs]
+        judge = None
     else:
-        raise ValueError("start is 'cold' or 'surrogate'")
+        raise ValueError("start is 'cold', 'physics' or 'surrogate'")
     kw = dict(tol=tol, check=check, max_steps=max_steps)
     nkw = dict(kw, max_steps=max_steps if narrow_max_steps is None else narrow_max_steps)
     batches = []

@@ -89,6 +89,9 @@ def _cases():
     # force off: the reference as shipped
     c["g16x12f"] = (lattice_params(16, 12, kappa_h=4.0, zeta=-2.0, ex=1e-3, force=False), 15, 100)
     c["config1"] = (lattice_params(256, 128, kappa_h=8.0, zeta=-2.0, ex=1e-4, diff=0.05), 0, 20000)
+    # speed only: the 4096x1024 channel's physics in FP64, 1000 steps of the
+    # reference's own loop (its "speed:" line) against the drop-in build
+    c["speed2"] = (lattice_params(4096, 1024, kappa_h=32.0, zeta=-4.0, ex=5e-5, diff=0.05), 1, 1000)
     return c
 
 

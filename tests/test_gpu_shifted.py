@@ -81,6 +81,29 @@ def test_fp32_pb_start_strong_wall():
     assert max(e.values()) <= 1e-5, e
 
 
+def test_fp32_config2_channel_all_rows():
+    """The 4096x1024 channel of the FP32 benchmark (kappa*H = 32, zeta = -4,
+    E_x = 5e-5), 10,000 steps from the seed-1 noisy uniform start, FP32
+    shifted storage (FP32 collision arithmetic) against the FP64 path:
+    u_x, c+, c-, psi within 1e-5 of the field's max-abs over every row, wall
+    rows included, and the plug velocity within 1e-5 of max |u_x|.
+    At 10,000 steps the centre has not accelerated yet (the viscous time
+    across the channel is ~6e6 steps): the plug is ~4e-10, 3e-7 of the
+    Helmholtz-Smoluchowski speed, and its error relative to itself (printed,
+    not asserted) sits near the rounding floor of FP32 storage."""
+    import ekpnp
+    w = ekpnp.WORKLOADS["channel-4096x1024"]
+    p = ekpnp.workload_params("channel-4096x1024")
+    init = ekpnp.noisy_uniform_state(w["nx"], w["ny"], w["seed"])
+    ref = run(p, init, w["steps"], ekpnp.STORE_F64)
+    got = run(p, init, w["steps"], ekpnp.STORE_F32)
+    e = errors(got, ref)
+    own = abs(plug(got["ux"]) - plug(ref["ux"])) / abs(plug(ref["ux"]))
+    print("FP32 vs FP64, 4096x1024, 10,000 steps:", e, "plug relative to itself:", own,
+          "plug / u_HS:", plug(ref["ux"]) / ekpnp.helmholtz_smoluchowski(p))
+    assert max(e.values()) <= 1e-5, e
+
+
 def test_fp16_storage_bounded(medium):
     """FP16 storage keeps 11 significant bits of each deviation: enough for
     c+-, psi and the plug velocity at the percent level, not for the small
