@@ -174,6 +174,8 @@ def run_ours(args, d):
 
     # ---- device-timed region ----
     ch = Channel(p)
+    if args.storage != "f64" and args.lbm_kernel != "auto":
+        ch.set_lbm_kernel(args.lbm_kernel)
     ch.set_fields(**init)
     ch.init_equilibrium()
     ch.step(args.warmup)
@@ -224,6 +226,8 @@ def run_ours(args, d):
     chunk = 100
     reps = max(1, args.steps // chunk)
     ch = Channel(p)
+    if args.storage != "f64" and args.lbm_kernel != "auto":
+        ch.set_lbm_kernel(args.lbm_kernel)
     ch.set_fields(**init)
     ch.init_equilibrium()
     ch.step(min(args.warmup, 10))
@@ -259,7 +263,7 @@ def run_ours(args, d):
             "data": "synthetic (seeded noisy uniform state, u = psi = 0)",
             "config": {"workload": args.workload, "nx": nx, "ny": ny, "storage": args.storage + "-shifted"
                        if args.storage != "f64" else "f64", "kappa_h": w["kappa_h"], "zeta": w["zeta"],
-                       "e_x": w["ex"], "parallelism": f"replicas x{d.world}",
+                       "e_x": w["ex"], "parallelism": f"replicas x{d.world}", "lbm_kernel": args.lbm_kernel,
                        "l2": "working set > 126 MB L2 (2 x 27 population planes), no flush"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
@@ -595,6 +599,8 @@ def main():
     ap.add_argument("--batch", action="store_true",
                     help="the batched workload (512 uneven channels) instead of one channel")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--lbm-kernel", choices=("auto", "plain", "tma", "prefetch"), default="auto",
+                    help="form of the shifted-storage LBM kernel (bit-identical forms)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -133,25 +133,27 @@ def test_fp32_wall_and_unit_variants(name):
 
 @pytest.mark.parametrize("shape", [(64, 20), (100, 17), (256, 40), (384, 33)], ids=lambda s: f"{s[0]}x{s[1]}")
 @pytest.mark.parametrize("storage", [1, 2], ids=["f32", "f16"])
-def test_tma_pipeline_bitwise_equals_plain(shape, storage):
-    """The TMA-fed pipeline and the plain per-node kernel run the same
-    collision: bit-identical fields after a first step (in-place reads),
-    wall rows, a partial last tile (nx % 128 != 0) and periodic wrap."""
+@pytest.mark.parametrize("form", ["tma", "prefetch"])
+def test_kernel_forms_bitwise_equal_plain(shape, storage, form):
+    """The TMA-fed pipeline, the tile-walking form with L2 prefetch and the
+    plain per-node kernel run the same collision: bit-identical fields after
+    a first step (in-place reads), wall rows, a partial last tile
+    (nx % 128 != 0) and periodic wrap."""
     import ekpnp
     nx, ny = shape
     p = ekpnp.channel_params(nx, ny, kappa_h=6.0, zeta=-1.5, zeta_hi=-1.0, ex=1e-3, uw=1e-3, storage=storage)
     init = ekpnp.noisy_uniform_state(nx, ny, seed=4)
     out = {}
-    for form in ("plain", "tma"):
+    for f in ("plain", form):
         with ekpnp.Channel(p) as ch:
-            ch.set_lbm_kernel(form)
+            ch.set_lbm_kernel(f)
             ch.set_fields(**init)
             ch.init_equilibrium()
             ch.step(1)
             first = ch.get_fields()
             ch.step(60)
             out[form] = (first, ch.get_fields())
-    for a, b in zip(out["plain"], out["tma"]):
+    for a, b in zip(out["plain"], out[form]):
         for k in a:
             assert np.array_equal(a[k], b[k]), k
 
