@@ -50,25 +50,50 @@ constexpr int REFS_TPB = 256;
 #ifndef EK_BATCH_SM_THREADS
 #define EK_BATCH_SM_THREADS 896
 #endif
+// Tiles are handed out from a queue, TILE_CHUNK consecutive tiles (same
+// channel, adjacent rows) at a time: queue[0] is the next unclaimed tile,
+// queue[1] counts the blocks that found the list empty; the last of them
+// puts both back to zero for the next launch (every other block has made its
+// last claim by then), so the queue needs no reset between launches or graph
+// replays.
+constexpr int TILE_CHUNK = 4;
+
 template <typename S, bool FIRST, bool EE, int TXB>
 __global__ void __launch_bounds__(TXB, (EK_BATCH_SM_THREADS / TXB) > 0 ? (EK_BATCH_SM_THREADS / TXB) : 1)
 batch_lbm(const ChanF *__restrict__ chans, const S *const *__restrict__ src, S *const *__restrict__ dst,
-          double *const *__restrict__ fields, const int4 *__restrict__ tiles, int ntiles, bool mom, int sbuf) {
+          double *const *__restrict__ fields, const int4 *__restrict__ tiles, int ntiles, int *__restrict__ queue,
+          bool mom, int sbuf) {
     __shared__ ChanF ks;
-    const int per = (ntiles + gridDim.x - 1) / gridDim.x;
-    const int t0 = blockIdx.x * per, t1 = min(ntiles, t0 + per);
+    __shared__ int claim;
     int cur = -1;
-    for (int t = t0; t < t1; ++t) {
-        const int4 tl = tiles[t];  // {channel, y0, x0, width}
-        if (tl.x != cur) {
-            __syncthreads();
-            if (threadIdx.x == 0) ks = chans[tl.x];
-            __syncthreads();
-            cur = tl.x;
+    for (;;) {
+        if (threadIdx.x == 0) claim = atomicAdd(queue, TILE_CHUNK);
+        __syncthreads();
+        const int t0 = claim;
+        if (t0 >= ntiles) break;  // the same for every thread of the block
+        const int t1 = min(ntiles, t0 + TILE_CHUNK);
+        for (int t = t0; t < t1; ++t) {
+            const int4 tl = tiles[t];  // {channel, y0, x0, width}
+            if (tl.x != cur) {
+                __syncthreads();
+                if (threadIdx.x == 0) ks = chans[tl.x];
+                __syncthreads();
+                cur = tl.x;
+            }
+            const int r = threadIdx.x / tl.w;
+            const int x = tl.z + (threadIdx.x - r * tl.w), y = tl.y + r;
+            if (x < ks.nx && y < ks.ny)
+                node_shifted<S, FIRST, EE>(ks, src[cur], dst[cur], fields[cur], x, y, mom, sbuf);
         }
-        const int r = threadIdx.x / tl.w;
-        const int x = tl.z + (threadIdx.x - r * tl.w), y = tl.y + r;
-        if (x < ks.nx && y < ks.ny) node_shifted<S, FIRST, EE>(ks, src[cur], dst[cur], fields[cur], x, y, mom, sbuf);
+        __syncthreads();  // every thread has read `claim` before thread 0 claims again
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(queue + 1, 1) == (int)gridDim.x - 1) {
+            queue[0] = 0;
+            queue[1] = 0;
+            __threadfence();
+        }
     }
 }
 
@@ -112,10 +137,11 @@ __global__ void batch_commit_refs(const ChanF *__restrict__ chans, float *const 
 
 template <typename S, int TXB>
 cudaError_t lbm_t(const ChanF *chans, const void *src, void *dst, double *const *fields, const int4 *tiles,
-                  int ntiles, int grid, bool first, bool ee, bool mom, int sbuf, cudaStream_t s) {
+                  int ntiles, int *queue, int grid, bool first, bool ee, bool mom, int sbuf, cudaStream_t s) {
     const S *const *a = (const S *const *)src;
     S *const *b = (S *const *)dst;
-#define EK_BL(F, E) batch_lbm<S, F, E, TXB><<<grid, TXB, 0, s>>>(chans, a, b, fields, tiles, ntiles, mom, sbuf)
+#define EK_BL(F, E) \
+    batch_lbm<S, F, E, TXB><<<grid, TXB, 0, s>>>(chans, a, b, fields, tiles, ntiles, queue, mom, sbuf)
     if (first) {
         if (ee) EK_BL(true, true);
         else EK_BL(true, false);
@@ -129,10 +155,12 @@ cudaError_t lbm_t(const ChanF *chans, const void *src, void *dst, double *const 
 
 template <typename S>
 cudaError_t lbm_s(int txb, const ChanF *chans, const void *src, void *dst, double *const *fields, const int4 *tiles,
-                  int ntiles, int grid, bool first, bool ee, bool mom, int sbuf, cudaStream_t s) {
-    if (txb == 64) return lbm_t<S, 64>(chans, src, dst, fields, tiles, ntiles, grid, first, ee, mom, sbuf, s);
-    if (txb == 256) return lbm_t<S, 256>(chans, src, dst, fields, tiles, ntiles, grid, first, ee, mom, sbuf, s);
-    return lbm_t<S, 128>(chans, src, dst, fields, tiles, ntiles, grid, first, ee, mom, sbuf, s);
+                  int ntiles, int *queue, int grid, bool first, bool ee, bool mom, int sbuf, cudaStream_t s) {
+    if (txb == 64)
+        return lbm_t<S, 64>(chans, src, dst, fields, tiles, ntiles, queue, grid, first, ee, mom, sbuf, s);
+    if (txb == 256)
+        return lbm_t<S, 256>(chans, src, dst, fields, tiles, ntiles, queue, grid, first, ee, mom, sbuf, s);
+    return lbm_t<S, 128>(chans, src, dst, fields, tiles, ntiles, queue, grid, first, ee, mom, sbuf, s);
 }
 
 template <typename S>
@@ -194,6 +222,7 @@ struct ek_batch {
     int4 *d_kq = nullptr;
     int4 *d_tiles = nullptr;
     int ntiles = 0, txb = 128, grid = 0;
+    int *d_queue = nullptr;          // LBM tile queue: next tile, finished blocks (zero between launches)
     int2 *d_pairs = nullptr;         // Poisson row-pair items
     int npairs = 0;
     int3 *d_modes = nullptr;         // Poisson x-mode items
@@ -258,13 +287,17 @@ int build_tiles(ek_batch *b, int txb) {
     release_graph(b);
     int rc = upload(&b->d_tiles, tiles, b->stream);
     if (rc != EK_OK) return rc;
+    if (!b->d_queue) {
+        EK_BCUDA(cudaMalloc(&b->d_queue, 2 * sizeof(int)), "tile queue");
+        EK_BCUDA(cudaMemsetAsync(b->d_queue, 0, 2 * sizeof(int), b->stream), "tile queue");
+    }
     b->ntiles = (int)tiles.size();
     b->txb = txb;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int occ = b->storage == EK_STORE_F16 ? lbm_occupancy<__half>(txb) : lbm_occupancy<float>(txb);
-    b->grid = std::max(1, std::min(b->ntiles, sms * occ));
+    b->grid = std::max(1, std::min((b->ntiles + TILE_CHUNK - 1) / TILE_CHUNK, sms * occ));
     return EK_OK;
 }
 
@@ -354,10 +387,10 @@ int launch_step(ek_batch *b, bool first, bool ee, bool mom) {
     const void *src = b->d_pops[b->cur];
     void *dst = b->d_pops[b->cur ^ 1];
     cudaError_t e = b->storage == EK_STORE_F16
-                        ? lbm_s<__half>(b->txb, b->d_chanf, src, dst, b->d_fields, b->d_tiles, b->ntiles, b->grid,
-                                        first, ee, mom, b->cur, b->stream)
-                        : lbm_s<float>(b->txb, b->d_chanf, src, dst, b->d_fields, b->d_tiles, b->ntiles, b->grid,
-                                       first, ee, mom, b->cur, b->stream);
+                        ? lbm_s<__half>(b->txb, b->d_chanf, src, dst, b->d_fields, b->d_tiles, b->ntiles,
+                                        b->d_queue, b->grid, first, ee, mom, b->cur, b->stream)
+                        : lbm_s<float>(b->txb, b->d_chanf, src, dst, b->d_fields, b->d_tiles, b->ntiles,
+                                       b->d_queue, b->grid, first, ee, mom, b->cur, b->stream);
     EK_BCUDA(e, "batch LBM kernel");
     EK_BCUDA(batch_poisson(0, b->d_plans, b->d_chan, b->d_fields, b->d_pairs, b->npairs, false, b->stream),
              "batch rows");
@@ -511,7 +544,7 @@ int ek_batch_destroy(ek_batch *b) {
     for (ek_ctx *c : b->ch) ek_destroy(c);  // the channels do not own the batch's stream
     void *tables[] = {b->d_chanf, b->d_chan,  b->d_plans,  b->d_pops[0],  b->d_pops[1], b->d_fields,
                       b->d_spare, b->d_kq,    b->d_tiles,  b->d_pairs,    b->d_modes,   b->d_rows,
-                      b->d_snaps, b->d_ritems, b->d_rranges, b->d_rpart,  b->d_zeros};
+                      b->d_snaps, b->d_ritems, b->d_rranges, b->d_rpart,  b->d_zeros, b->d_queue};
     for (void *t : tables)
         if (t) cudaFree(t);
     if (b->fork) cudaEventDestroy(b->fork);

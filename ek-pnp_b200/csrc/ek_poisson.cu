@@ -619,8 +619,9 @@ inv_rows_r16f(const PoissonPlan pp, const Chan c, double *__restrict__ psi, bool
 // registers with its pivots.  The forward recurrence
 // d_j = (dy^2 S_j - d_{j-1}) piv_j is linear in the value entering a segment,
 // so each segment first runs with a zero entry value while accumulating the
-// product of (-piv); one thread per mode then carries the true entry values
-// across the S segments through shared memory, and each segment adds its
+// product of (-piv); the true entry values follow from composing the
+// segments' affine maps D -> e + f D in order, a log2(S)-round scan over the
+// segments of each mode in shared memory, and each segment adds its
 // correction.  The backward recurrence x_j = d_j - piv_j x_{j+1} is split the
 // same way.  The result is the Thomas solution, reassociated.
 constexpr int TB_THREADS = 512;
@@ -629,16 +630,43 @@ constexpr int TB_L = 16;
 template <typename R, typename C> struct TridiagSharedT {
     C ends[TB_THREADS];
     R mults[TB_THREADS];
-    C carry[TB_THREADS];
 };
 using TridiagShared = TridiagSharedT<double, double2>;
+
+// Value entering this thread's segment: the affine maps D -> e + f D of the
+// segments of its mode (the block's threads are seg * M + mode) composed in
+// order -- forward from segment 0 (FWD) or backward from segment S-1 -- by a
+// Kogge-Stone scan over the S segments in shared memory (log2 S rounds); the
+// first segment in that order enters with 0.  Every thread of the block
+// calls it.
+template <bool FWD, typename R, typename C>
+__device__ __forceinline__ C seg_carry(C e, R f, int seg, int S, int M, TridiagSharedT<R, C> &sh) {
+    const int tid = threadIdx.x, mode = tid - seg * M;
+    for (int off = 1; off < S; off <<= 1) {
+        sh.ends[tid] = e;
+        sh.mults[tid] = f;
+        __syncthreads();
+        const int src = FWD ? seg - off : seg + off;
+        if (FWD ? src >= 0 : src < S) {
+            const C e2 = sh.ends[src * M + mode];
+            const R f2 = sh.mults[src * M + mode];
+            e = cmake<C>(e.x + f * e2.x, e.y + f * e2.y);  // this segment after the earlier ones
+            f = f * f2;
+        }
+        __syncthreads();
+    }
+    sh.ends[tid] = e;
+    __syncthreads();
+    const int prev = FWD ? seg - 1 : seg + 1;
+    const C out = (FWD ? prev >= 0 : prev < S) ? sh.ends[prev * M + mode] : cmake<C>(0.0, 0.0);
+    __syncthreads();  // sh is written again by the next call
+    return out;
+}
 
 // One block of the partitioned solve on a spectrum of type C (pivots R).
 template <typename R, typename C>
 __device__ __forceinline__ void tridiag_part_gen(const R *__restrict__ piv, C *__restrict__ spec, int n, int nx,
                                                  size_t mp, R dy2, int M, int m_base, TridiagSharedT<R, C> &sh) {
-    C *ends = sh.ends, *carry = sh.carry;
-    R *mults = sh.mults;
     const int mlast = nx / 2;
     const int tid = threadIdx.x, mode = tid % M, seg = tid / M, S = TB_THREADS / M;
     const int m = m_base + mode;
@@ -663,21 +691,8 @@ __device__ __forceinline__ void tridiag_part_gen(const R *__restrict__ piv, C *_
             v[q] = d;
         }
     }
-    ends[tid] = d;
-    mults[tid] = mu;
-    __syncthreads();
-    if (seg == 0) {  // true entry value of every segment
-        C D = cmake<C>(0.0, 0.0);
-        for (int s_ = 0; s_ < S; ++s_) {
-            carry[s_ * M + mode] = D;
-            const C e = ends[s_ * M + mode];
-            const R f = mults[s_ * M + mode];
-            D = cmake<C>(e.x + f * D.x, e.y + f * D.y);
-        }
-    }
-    __syncthreads();
     {
-        const C D = carry[tid];
+        const C D = seg_carry<true>(d, mu, seg, S, M, sh);  // true entry value of the segment
         mu = R(1);
 #pragma unroll
         for (int q = 0; q < TB_L; ++q) {
@@ -698,22 +713,8 @@ __device__ __forceinline__ void tridiag_part_gen(const R *__restrict__ piv, C *_
             v[q] = x;
         }
     }
-    __syncthreads();  // carries of the forward sweep are no longer read
-    ends[tid] = x;
-    mults[tid] = nu;
-    __syncthreads();
-    if (seg == 0) {  // true exit value of every segment (x_n = 0)
-        C X = cmake<C>(0.0, 0.0);
-        for (int s_ = S - 1; s_ >= 0; --s_) {
-            carry[s_ * M + mode] = X;
-            const C e = ends[s_ * M + mode];
-            const R f = mults[s_ * M + mode];
-            X = cmake<C>(e.x + f * X.x, e.y + f * X.y);
-        }
-    }
-    __syncthreads();
+    const C X = seg_carry<false>(x, nu, seg, S, M, sh);  // true exit value of the segment (x_n = 0)
     if (!mvalid) return;
-    const C X = carry[tid];
     nu = R(1);
 #pragma unroll
     for (int q = TB_L - 1; q >= 0; --q) {

@@ -152,7 +152,7 @@ def test_kernel_forms_bitwise_equal_plain(shape, storage, form):
             ch.step(1)
             first = ch.get_fields()
             ch.step(60)
-            out[form] = (first, ch.get_fields())
+            out[f] = (first, ch.get_fields())
     for a, b in zip(out["plain"], out[form]):
         for k in a:
             assert np.array_equal(a[k], b[k]), k
