@@ -361,6 +361,49 @@ def _start_summary(r, cap):
             "mean_steps_capped": float(np.mean(np.where(ok, st, cap)))}
 
 
+def ws_training_set(n_train, gen_cap, check):
+    """Steady states of the training channels (seed 3, 16 columns each) from
+    the batched solver: loaded from EK_WS_CACHE when that file exists (written
+    by an earlier run of this same function), else generated and, with
+    EK_WS_CACHE set, saved there.  Returns (specs, targets, converged, steps,
+    generation seconds)."""
+    from ekpnp import batch_specs, warmstart as ws
+    t0 = time.perf_counter()
+    tr = batch_specs(n_train, seed=3)
+    cache = os.environ.get("EK_WS_CACHE")
+    if cache and os.path.exists(cache):
+        z = np.load(cache)
+        if len(z["T"]) != n_train:
+            raise RuntimeError(f"{cache} holds {len(z['T'])} channels, not {n_train}")
+        T, conv, steps = z["T"], z["conv"], z["steps"]
+    else:
+        T, conv, info = ws.generate_steady_states(tr, nx=16, max_steps=gen_cap, check=check)
+        steps = info["steps"]
+        if cache:
+            np.savez(cache, T=T, conv=conv, steps=steps)
+    return tr, T, conv, steps, time.perf_counter() - t0
+
+
+def steps_to_tol(hist, check, tol=1e-8):
+    """Steps at which a residual history (one value every `check` steps)
+    reaches tol: the first check below it, else the log-linear extrapolation
+    of the later half of the history (None where it does not decrease)."""
+    h = np.asarray(hist, dtype=np.float64)
+    s = check * (np.arange(len(h)) + 1)
+    below = np.nonzero(np.isfinite(h) & (h < tol))[0]
+    if len(below):
+        return {"steps": int(s[below[0]]), "extrapolated": False}
+    k = len(h) // 2
+    ok = np.isfinite(h[k:]) & (h[k:] > 0)
+    if ok.sum() < 2:
+        return None
+    slope, icpt = np.polyfit(s[k:][ok], np.log(h[k:][ok]), 1)
+    if slope >= 0:
+        return None
+    return {"steps": int((np.log(tol) - icpt) / slope), "extrapolated": True,
+            "decay_per_100k_steps": float(np.exp(slope * 1e5))}
+
+
 def run_warmstart(args, d):
     """Learned warm start: steady states of `train` channels (seed 3) from the
     batched solver, the network trained on them (tensor-core kernels), then
@@ -376,18 +419,7 @@ def run_warmstart(args, d):
     cap = env_int("EK_WS_CAP", 200_000)
     gen_cap = env_int("EK_WS_GEN_CAP", 120_000)
     check = 2000
-    t0 = time.perf_counter()
-    tr = batch_specs(n_train, seed=3)
-    cache = os.environ.get("EK_WS_CACHE")
-    if cache and os.path.exists(cache):
-        z = np.load(cache)
-        T, conv, gen_steps = z["T"], z["conv"], z["steps"]
-    else:
-        T, conv, info = ws.generate_steady_states(tr, nx=16, max_steps=gen_cap, check=check)
-        gen_steps = info["steps"]
-        if cache:
-            np.savez(cache, T=T, conv=conv, steps=gen_steps)
-    gen_s = time.perf_counter() - t0
+    tr, T, conv, gen_steps, gen_s = ws_training_set(n_train, gen_cap, check)
     ok = np.all(np.isfinite(T), axis=1)
     trs = [s for s, o in zip(tr, ok) if o]
     ev = batch_specs(n_eval, seed=4)
@@ -458,14 +490,21 @@ def run_warmstart(args, d):
 
 def run_hetero(args, d):
     """Heterogeneous wall: one 8192 x 2048 channel, zeta(x) = -2 + 1.5 sin(2 pi x / 1024),
-    kappa*H = 64, E_x = 1e-4, seed 5.  FP32 shifted from a warm start (the
-    residual surrogate at the mean zeta when a training cache is given in
-    EK_WS_CACHE, else the per-column Poisson-Boltzmann/electro-osmotic physics
-    start) against the FP64 path from the uniform cold start: MLUPS, LBM
-    roofline, FP32 error against FP64 from the same start, residual after a
-    step cap."""
+    kappa*H = 64, E_x = 1e-4, seed 5.  Arms, each stepped to residual < 1e-8
+    or the step cap (EK_HET_CAP), residual checked every 1000 steps:
+      f32_surrogate  FP32 shifted from the residual surrogate evaluated at the
+                     mean zeta (trained here on the batched solver's steady
+                     states, ws_training_set),
+      f32_physics    FP32 shifted from the per-column Poisson-Boltzmann ions
+                     and potential with the electro-osmotic velocity (the start
+                     without the network),
+      f64_cold       the FP64 path from the uniform noisy cold start.
+    Reports MLUPS, the LBM roofline, the FP32 error against the FP64 path from
+    the same start after the timed steps, steps and wall time to the cap, the
+    final residual and, where the cap came first, the steps to 1e-8
+    extrapolated from the residual's decay (steps_to_tol)."""
     import ekpnp
-    from ekpnp import Channel, channel_params, noisy_uniform_state, warmstart as ws
+    from ekpnp import Channel, noisy_uniform_state, warmstart as ws
     if d.rank != 0:
         return 0
     ekpnp.set_device(d.local)
@@ -478,6 +517,7 @@ def run_hetero(args, d):
     zeta = -2.0 + 1.5 * np.sin(2 * np.pi * x / 1024.0)
     walls = dict(zeta_lo=zeta, zeta_hi=zeta, cp_lo=np.exp(-zeta), cp_hi=np.exp(-zeta), cn_lo=np.exp(zeta),
                  cn_hi=np.exp(zeta))
+    peak, peak_kind = measured_peak_gbs()
 
     def make(storage):
         p = ekpnp.spec_params(spec, storage)
@@ -487,99 +527,107 @@ def run_hetero(args, d):
             ch.set_rebase_interval(200)
         return ch
 
-    # warm start fields
-    cache = os.environ.get("EK_WS_CACHE")
-    if cache and os.path.exists(cache):
-        from ekpnp import batch_specs
-        z = np.load(cache)
-        tr = batch_specs(len(z["T"]), seed=3)
-        ok = np.all(np.isfinite(z["T"]), axis=1)
-        sg = ws.Surrogate("residual", seed=7)
-        sg.fit([s_ for s_, o in zip(tr, ok) if o], z["T"][ok], iters=12000, lr=2e-3)
-        warm = sg.fields([spec])[0]
-        sg.close()
-        start_kind = "residual surrogate at the mean zeta"
-    else:
-        with make(ekpnp.STORE_F32) as ch:
-            ch.init_poisson_boltzmann("newton")
-            warm = ch.get_fields(("rho", "ux", "uy", "cp", "cn", "psi"))
-        u = ws.u_hs(ekpnp.spec_params(spec, 0)) / spec["zeta"] * (zeta[None, :] - warm["psi"])
-        warm["ux"] = u
-        start_kind = "per-column Poisson-Boltzmann + electro-osmotic velocity"
+    # ---- starts ----
+    starts = {}
+    n_train = env_int("EK_WS_TRAIN", 8192)
+    tr, T, conv, _, gen_s = ws_training_set(n_train, env_int("EK_WS_GEN_CAP", 120_000), 2000)
+    ok = np.all(np.isfinite(T), axis=1)
+    sg = ws.Surrogate("residual", seed=7)
+    t1 = time.perf_counter()
+    sg.fit([s_ for s_, o in zip(tr, ok) if o], T[ok], iters=env_int("EK_WS_ITERS", 12000), lr=2e-3)
+    train_s = time.perf_counter() - t1
+    t1 = time.perf_counter()
+    starts["f32_surrogate"] = sg.fields([spec])[0]
+    infer_s = time.perf_counter() - t1
+    sg.close()
+    t1 = time.perf_counter()
+    with make(ekpnp.STORE_F32) as ch:
+        ch.init_poisson_boltzmann("newton")
+        phys = ch.get_fields(("rho", "ux", "uy", "cp", "cn", "psi"))
+    phys["ux"] = ws.u_hs(ekpnp.spec_params(spec, 0)) / spec["zeta"] * (zeta[None, :] - phys["psi"])
+    starts["f32_physics"] = phys
+    phys_s = time.perf_counter() - t1
 
-    def timed_run(ch, steps):
+    def timed(ch, steps):
         ch.sync()
         ch.mark(0)
         ch.step(steps)
         ch.mark(1)
-        ms = ch.elapsed_ms(0, 1)
-        return ms
+        return ch.elapsed_ms(0, 1)
 
-    out = {}
-    # FP32 from the warm start: MLUPS, roofline, then to the cap
-    with make(ekpnp.STORE_F32) as ch:
-        ch.set_fields(**warm)
-        ch.init_equilibrium()
-        ch.step(args.warmup)
-        ms = timed_run(ch, K)
-        ch.profile(True)
-        ch.step(min(K, 200))
-        prof = ch.profile_read()
-        ch.profile(False)
-        f32_k = ch.get_fields(("ux", "cp", "cn", "psi"))
-        lbm_ms, lbm_n = prof["lbm"]
-        per = lbm_ms / max(lbm_n, 1) / 1e3
-        peak, kind = measured_peak_gbs()
-        out["f32_warm"] = {"mlups": nx * ny * K / (ms / 1e3) / 1e6, "ms_per_step": ms / K,
-                           "lbm_launch_ms": per * 1e3, "lbm_gbs": nx * ny * 232 / per / 1e9,
-                           "lbm_frac": nx * ny * 232 / per / 1e9 / peak, "peak_kind": kind}
-        t0 = time.perf_counter()
-        ch.residual(check)
-        hist = []
-        while ch.steps < cap:
-            ch.step(check)
-            hist.append(float(ch.residual(check)[4]))
-            if hist[-1] < 1e-8:
-                break
-        out["f32_warm"].update({"steps": int(ch.steps), "residual": hist[-1] if hist else None,
-                                "wall_s": time.perf_counter() - t0})
-    # FP64 from the same warm start: error of FP32 after K + warmup + 200 steps
-    with make(ekpnp.STORE_F64) as ch:
-        ch.set_fields(**warm)
-        ch.init_equilibrium()
-        ch.step(args.warmup + K + min(K, 200))
-        f64_k = ch.get_fields(("ux", "cp", "cn", "psi"))
-    out["f32_error_vs_f64"] = {k: float(np.abs(f32_k[k] - f64_k[k]).max() / np.abs(f64_k[k]).max())
-                               for k in f64_k}
-    # FP64 from the uniform cold start
-    with make(ekpnp.STORE_F64) as ch:
-        ch.set_fields(**noisy_uniform_state(nx, ny, seed=5))
-        ch.init_equilibrium()
-        ch.step(args.warmup)
-        ms = timed_run(ch, K)
-        out["f64_cold"] = {"mlups": nx * ny * K / (ms / 1e3) / 1e6, "ms_per_step": ms / K}
+    def to_steady(ch):
         t0 = time.perf_counter()
         ch.residual(check)
         hist = []
         while ch.steps < cap:
             ch.step(check)
             try:
-                r = ch.residual(check)[4]
-            except ekpnp.EkError:  # non-finite fields: the cold start diverged
+                r = float(ch.residual(check)[4])
+            except ekpnp.EkError:  # non-finite fields: the run diverged
                 r = float("nan")
-            hist.append(float(r))
+            hist.append(r)
             if not np.isfinite(r) or r < 1e-8:
                 break
-        out["f64_cold"].update({"steps": int(ch.steps), "residual": hist[-1] if hist else None,
-                                "wall_s": time.perf_counter() - t0})
-    line = {"metric": "coupled_mlups", "value": out["f32_warm"]["mlups"], "unit": "MLUPS", "n_gpus": 1,
-            "steps": K, "warmup": args.warmup, "ms_per_step": out["f32_warm"]["ms_per_step"],
+        return {"steps": int(ch.steps), "residual": hist[-1] if hist else None,
+                "wall_s": time.perf_counter() - t0, "to_1e-8": steps_to_tol(hist, check),
+                "residual_every_10k": hist[9::10]}
+
+    out = {}
+    f32_k = {}
+    for arm in ("f32_surrogate", "f32_physics"):
+        with make(ekpnp.STORE_F32) as ch:
+            ch.set_fields(**starts[arm])
+            ch.init_equilibrium()
+            ch.step(args.warmup)
+            ms = timed(ch, K)
+            ch.profile(True)
+            ch.step(min(K, 200))
+            prof = ch.profile_read()
+            ch.profile(False)
+            f32_k[arm] = ch.get_fields(("ux", "cp", "cn", "psi"))
+            lbm_ms, lbm_n = prof["lbm"]
+            per = lbm_ms / max(lbm_n, 1) / 1e3
+            out[arm] = {"mlups": nx * ny * K / (ms / 1e3) / 1e6, "ms_per_step": ms / K,
+                        "lbm_launch_ms": per * 1e3, "lbm_gbs": nx * ny * 224 / per / 1e9,
+                        "lbm_frac": nx * ny * 224 / per / 1e9 / peak, "peak_kind": peak_kind,
+                        "step_frac": nx * ny * K / (ms / 1e3) * 248 / 1e9 / peak}
+            out[arm].update(to_steady(ch))
+    # FP32 error against the FP64 path from the surrogate start (same steps)
+    with make(ekpnp.STORE_F64) as ch:
+        ch.set_fields(**starts["f32_surrogate"])
+        ch.init_equilibrium()
+        ch.step(args.warmup + K + min(K, 200))
+        f64_k = ch.get_fields(("ux", "cp", "cn", "psi"))
+    err = {k: float(np.abs(f32_k["f32_surrogate"][k] - f64_k[k]).max() / np.abs(f64_k[k]).max()) for k in f64_k}
+    c = ny // 4
+    plug = lambda u: float(u[c:ny - c].mean())
+    err["plug"] = abs(plug(f32_k["f32_surrogate"]["ux"]) - plug(f64_k["ux"])) / np.abs(f64_k["ux"]).max()
+    # FP64 from the uniform cold start
+    with make(ekpnp.STORE_F64) as ch:
+        ch.set_fields(**noisy_uniform_state(nx, ny, seed=5))
+        ch.init_equilibrium()
+        ch.step(args.warmup)
+        ms = timed(ch, K)
+        out["f64_cold"] = {"mlups": nx * ny * K / (ms / 1e3) / 1e6, "ms_per_step": ms / K}
+        out["f64_cold"].update(to_steady(ch))
+    est = {a: (out[a]["to_1e-8"] or {}).get("steps") for a in out}
+    wall_est = {a: est[a] * out[a]["ms_per_step"] / 1e3 if est[a] else None for a in out}
+    line = {"metric": "coupled_mlups", "value": out["f32_surrogate"]["mlups"], "unit": "MLUPS", "n_gpus": 1,
+            "steps": K, "warmup": args.warmup, "ms_per_step": out["f32_surrogate"]["ms_per_step"],
             "higher_is_better": True, "scaling": "none", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seed 5 noise for the cold start)",
+            "data": "synthetic (seed 5 noise for the cold start; training channels seed 3)",
             "config": {"workload": f"hetero-wall-{nx}x{ny}", "kappa_h": 64.0, "e_x": 1e-4,
                        "zeta": "-2 + 1.5 sin(2 pi x / 1024)", "eps": 0.01, "rest_quirk": False,
-                       "warm_start": start_kind, "cap_steps": cap, "tol": 1e-8},
-            **out}
+                       "cap_steps": cap, "tol": 1e-8, "check_every": check, "train_channels": n_train,
+                       "train_usable": int(ok.sum())},
+            "start_seconds": {"training_set": gen_s, "training": train_s, "surrogate_inference": infer_s,
+                              "physics_start": phys_s},
+            **out,
+            "f32_error_vs_f64": err,
+            "time_to_1e-8_s": wall_est,
+            "time_to_1e-8_speedup_vs_f64_cold": {a: (wall_est["f64_cold"] / wall_est[a])
+                                                 if wall_est[a] and wall_est["f64_cold"] else None
+                                                 for a in ("f32_surrogate", "f32_physics")}}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -599,7 +647,7 @@ def main():
     ap.add_argument("--batch", action="store_true",
                     help="the batched workload (512 uneven channels) instead of one channel")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--lbm-kernel", choices=("auto", "plain", "tma", "prefetch"), default="auto",
+    ap.add_argument("--lbm-kernel", choices=("auto", "plain", "tma"), default="auto",
                     help="form of the shifted-storage LBM kernel (bit-identical forms)")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -919,7 +919,7 @@ int ek_step(ek_ctx *c, int32_t nsteps) {
                                        c->pops[c->cur ^ 1], c->fields, c->state_pre, ee, mom, c->cur, c->err_dev,
                                        c->wait_cycles, c->stream);
             return launch_step_shifted(c->chan, c->p.storage, c->pops[c->cur], c->pops[c->cur ^ 1], c->fields,
-                                       c->state_pre, ee, mom, c->cur, c->lbm_kernel == 3, c->stream);
+                                       c->state_pre, ee, mom, c->cur, c->stream);
         });
         if (rc0 != EK_OK) return rc0;
         c->cur ^= 1;
@@ -1013,7 +1013,7 @@ int ek_sync(ek_ctx *c) {
 int ek_set_option(ek_ctx *c, int32_t option, int64_t value) {
     if (!c) return fail(EK_ERR_INVALID, "null context");
     if (option == EK_OPT_LBM_KERNEL) {
-        if (value < 0 || value > 3) return fail(EK_ERR_INVALID, "EK_OPT_LBM_KERNEL takes 0, 1, 2 or 3");
+        if (value < 0 || value > 2) return fail(EK_ERR_INVALID, "EK_OPT_LBM_KERNEL takes 0, 1 or 2");
         if (value == 2 && !(shifted(c) && c->tma_ok))
             return fail(EK_ERR_UNSUPPORTED, "TMA-fed kernel needs shifted storage and a tensor map");
         c->lbm_kernel = (int)value;

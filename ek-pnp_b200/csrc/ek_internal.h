@@ -157,11 +157,8 @@ cudaError_t launch_pb_relax(const Chan &c, double omega, double *fields, double 
 // ---- shifted-storage forms (ek_lbm_f32.cu); storage = EK_STORE_F32 or _F16 ----
 // sbuf: index (0/1) of the population buffer that src is (it names the wall
 // ions' frames); buf: the buffer that pops is.
-// persistent: the tile-walking form with L2 bulk prefetch of the next tile
-// (step_shifted_pf); same bits as the one-tile-per-block form.
 cudaError_t launch_step_shifted(const Chan &c, int storage, const void *src, void *dst, double *fields,
-                                bool first, bool explicit_e, bool moments, int sbuf, bool persistent,
-                                cudaStream_t s);
+                                bool first, bool explicit_e, bool moments, int sbuf, cudaStream_t s);
 cudaError_t launch_init_shifted(const Chan &c, int storage, void *pops, const double *fields, bool explicit_e,
                                 int buf, cudaStream_t s);
 // Wall frames of the ions from the fields' wall rows (initialisation; buf is

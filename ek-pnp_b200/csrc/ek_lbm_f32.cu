@@ -89,71 +89,6 @@ step_shifted(const ChanF k, const S *__restrict__ src, S *__restrict__ dst, doub
     node_shifted<S, FIRST, EE>(k, src, dst, fields, x, blockIdx.y, mom, sbuf);
 }
 
-// Bulk prefetch of [p, p + bytes) into L2 by the copy engine: no registers,
-// no shared memory, nothing to wait for.  p 16-byte aligned, bytes a
-// multiple of 16, the range inside the allocation.
-__device__ __forceinline__ void l2_prefetch(const void *p, unsigned bytes) {
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-
-// L2 prefetch of what tile (y, x0) of step_shifted_pf will load: lane d < 27
-// of the calling warp takes population plane d (species-major), the row it
-// pulls from (own row on the first step and for the wall rows' ions), columns
-// [x0 - H, x0 + TPB + H) clamped to the padded row, H = 16 bytes of elements;
-// lanes 27..29 take the psi fluctuation rows y-1, y, y+1 (E's stencil).  The
-// one element that the x-wrap pulls from the far end of a row is left to the
-// demand load.  Every range starts on a 16-byte boundary (x0 is a multiple
-// of TPB, rows are nxp elements with nxp a multiple of 32) and ends at most
-// at the end of its row.
-template <typename S, bool FIRST>
-__device__ __forceinline__ void prefetch_tile(const ChanF &k, const S *__restrict__ src, int y, int x0, int lane) {
-    constexpr int H = 16 / (int)sizeof(S);
-    const int xa = max(x0 - H, 0), xb = min(x0 + TPB + H, k.nxp);
-    if (lane < 27) {
-        const int s = lane / 9, d = lane - 9 * s;
-        const bool wall = y == 0 || y == k.ny - 1;
-        int ys = y;
-        if (!FIRST && !(s > 0 && wall)) {
-            const int cy = cyd(d);
-            ys = y - cy;
-            if (ys < 0) ys += k.ny;
-            if (ys >= k.ny) ys -= k.ny;
-        }
-        const S *row = src + (size_t)lane * k.plane + (size_t)ys * k.nxp;
-        l2_prefetch(row + xa, (unsigned)((xb - xa) * sizeof(S)));
-    } else if (lane < 30) {
-        int ys = y + (lane - 28);
-        if (ys < 0 || ys >= k.ny) return;
-        const int fa = max(x0 - 4, 0), fb = min(x0 + TPB + 4, k.nxp);
-        l2_prefetch(k.psif + (size_t)ys * k.nxp + fa, (unsigned)((fb - fa) * sizeof(float)));
-    }
-}
-
-// Persistent form of step_shifted: each block walks the tiles (one row
-// segment of TPB columns) t = blockIdx.x, blockIdx.x + gridDim.x, ... and,
-// before each tile, has its first warp ask L2 for the populations of its
-// next tile.  The prefetches keep DRAM busy with no registers held, so the
-// demand loads that follow one tile later mostly hit L2.  Same node
-// function, so the same bits as step_shifted.
-template <typename S, bool FIRST, bool EE>
-__global__ void __launch_bounds__(TPB, EK_LBM_MIN_BLOCKS)
-step_shifted_pf(const ChanF k, const S *__restrict__ src, S *__restrict__ dst, double *__restrict__ fields, bool mom,
-                int sbuf, int xtiles, int ntiles) {
-    int t = blockIdx.x;
-    if (threadIdx.x < 32 && t < ntiles) {
-        const int tn = t;  // the first tile: nothing earlier to overlap it with, ask anyway
-        prefetch_tile<S, FIRST>(k, src, tn / xtiles, (tn % xtiles) * TPB, threadIdx.x);
-    }
-    for (; t < ntiles; t += gridDim.x) {
-        const int tn = t + gridDim.x;
-        if (threadIdx.x < 32 && tn < ntiles)
-            prefetch_tile<S, FIRST>(k, src, tn / xtiles, (tn % xtiles) * TPB, threadIdx.x);
-        const int y = t / xtiles;
-        const int x = (t - y * xtiles) * TPB + threadIdx.x;
-        if (x < k.nx) node_shifted<S, FIRST, EE>(k, src, dst, fields, x, y, mom, sbuf);
-    }
-}
-
 template <typename S>
 __global__ void __launch_bounds__(TPB)
 init_shifted(const ChanF k, S *__restrict__ pops, const double *__restrict__ fields, bool explicit_e, int buf) {
@@ -174,51 +109,12 @@ __global__ void __launch_bounds__(256) wall_delta(const ChanF k, const float *__
     if (i < 4 * k.nx) wall_delta_dev(k, kwall, wdelta, i);
 }
 
-// Resident blocks of step_shifted_pf on the current device (the grid of the
-// persistent form), looked up once per device and storage type.
-template <typename S>
-cudaError_t pf_grid(int *out) {
-    static int cache[2][64];
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-    int &g = cache[sizeof(S) == 2][dev];
-    if (g == 0) {
-        int sms = 0, per = 0;
-        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (e == cudaSuccess)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, step_shifted_pf<S, false, false>, TPB, 0);
-        if (e != cudaSuccess) return e;
-        g = max(1, per) * sms;
-    }
-    *out = g;
-    return cudaSuccess;
-}
-
 template <typename S>
 cudaError_t step_typed(const ChanF &k, const void *src, void *dst, double *fields, bool first, bool ee,
-                       bool mom, int sbuf, bool persistent, cudaStream_t s) {
+                       bool mom, int sbuf, cudaStream_t s) {
     const dim3 g((k.nx + TPB - 1) / TPB, k.ny);
     const S *a = (const S *)src;
     S *b = (S *)dst;
-    if (persistent) {
-        int grid = 0;
-        cudaError_t e = pf_grid<S>(&grid);
-        if (e != cudaSuccess) return e;
-        const int xt = (int)g.x, nt = (int)g.x * k.ny;
-        grid = min(grid, nt);
-#define EK_PF(F, E) step_shifted_pf<S, F, E><<<grid, TPB, 0, s>>>(k, a, b, fields, mom, sbuf, xt, nt)
-        if (first) {
-            if (ee) EK_PF(true, true);
-            else EK_PF(true, false);
-        } else {
-            if (ee) EK_PF(false, true);
-            else EK_PF(false, false);
-        }
-#undef EK_PF
-        return cudaGetLastError();
-    }
     if (first) {
         if (ee) step_shifted<S, true, true><<<g, TPB, 0, s>>>(k, a, b, fields, mom, sbuf);
         else step_shifted<S, true, false><<<g, TPB, 0, s>>>(k, a, b, fields, mom, sbuf);
@@ -322,12 +218,10 @@ cudaError_t launch_rebase(const Chan &c, int storage, void *pops, const float *k
 }
 
 cudaError_t launch_step_shifted(const Chan &c, int storage, const void *src, void *dst, double *fields,
-                                bool first, bool explicit_e, bool moments, int sbuf, bool persistent,
-                                cudaStream_t s) {
+                                bool first, bool explicit_e, bool moments, int sbuf, cudaStream_t s) {
     const ChanF k = make_chanf(c);
-    if (storage == EK_STORE_F16)
-        return step_typed<__half>(k, src, dst, fields, first, explicit_e, moments, sbuf, persistent, s);
-    return step_typed<float>(k, src, dst, fields, first, explicit_e, moments, sbuf, persistent, s);
+    if (storage == EK_STORE_F16) return step_typed<__half>(k, src, dst, fields, first, explicit_e, moments, sbuf, s);
+    return step_typed<float>(k, src, dst, fields, first, explicit_e, moments, sbuf, s);
 }
 
 cudaError_t launch_init_shifted(const Chan &c, int storage, void *pops, const double *fields, bool explicit_e,

@@ -121,9 +121,8 @@ class Channel:
         check(lib().ek_step(self._h, int(n)))
 
     def set_lbm_kernel(self, form):
-        """'auto', 'plain', 'tma' or 'prefetch' (shifted storage; all forms are
-        bit-identical)."""
-        check(lib().ek_set_option(self._h, 1, {"auto": 0, "plain": 1, "tma": 2, "prefetch": 3}[form]))
+        """'auto', 'plain' or 'tma' (shifted storage; both forms are bit-identical)."""
+        check(lib().ek_set_option(self._h, 1, {"auto": 0, "plain": 1, "tma": 2}[form]))
 
     def save_restart(self, path, time=0.0):
         """The channel's fields as the reference's data_end.dat (save_data_end)."""

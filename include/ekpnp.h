@@ -193,9 +193,7 @@ int ek_set_rebase_interval(ek_ctx *ctx, int32_t steps);
 /* Tuning options (ek_set_option).  EK_OPT_LBM_KERNEL selects the form of the
  * shifted-storage LBM kernel: 0 = automatic (currently the plain form, the
  * faster one on B200), 1 = plain per-node loads, 2 = TMA-fed pipeline
- * (producer warp + mbarrier ring of tensor copies), 3 = plain loads in
- * resident blocks that walk the row segments and ask L2 for the next
- * segment's populations ahead of time (bulk L2 prefetch).  All forms give
+ * (producer warp + mbarrier ring of tensor copies).  Both forms give
  * bit-identical results.  Returns EK_ERR_UNSUPPORTED for a form that this
  * context cannot run. */
 enum { EK_OPT_LBM_KERNEL = 1, EK_OPT_POISSON = 2, EK_OPT_LAST_STEP_MOMENTS = 3, EK_OPT_WAIT_CYCLES = 4 };

@@ -133,12 +133,11 @@ def test_fp32_wall_and_unit_variants(name):
 
 @pytest.mark.parametrize("shape", [(64, 20), (100, 17), (256, 40), (384, 33)], ids=lambda s: f"{s[0]}x{s[1]}")
 @pytest.mark.parametrize("storage", [1, 2], ids=["f32", "f16"])
-@pytest.mark.parametrize("form", ["tma", "prefetch"])
+@pytest.mark.parametrize("form", ["tma"])
 def test_kernel_forms_bitwise_equal_plain(shape, storage, form):
-    """The TMA-fed pipeline, the tile-walking form with L2 prefetch and the
-    plain per-node kernel run the same collision: bit-identical fields after
-    a first step (in-place reads), wall rows, a partial last tile
-    (nx % 128 != 0) and periodic wrap."""
+    """The TMA-fed pipeline and the plain per-node kernel run the same
+    collision: bit-identical fields after a first step (in-place reads), wall
+    rows, a partial last tile (nx % 128 != 0) and periodic wrap."""
     import ekpnp
     nx, ny = shape
     p = ekpnp.channel_params(nx, ny, kappa_h=6.0, zeta=-1.5, zeta_hi=-1.0, ex=1e-3, uw=1e-3, storage=storage)
