@@ -305,7 +305,8 @@ def run_batch(args, d):
     nn = b.nodes
     for ch in b:
         ch.init_poisson_boltzmann("newton")
-    b.set_cycle(200)
+    graph = env_int("EK_BATCH_GRAPH", 1) != 0
+    b.set_cycle(200, graph=graph)
     b.init_equilibrium()
     chosen, tune_ms = b.autotune(10)
     b.step(args.warmup)
@@ -339,8 +340,11 @@ def run_batch(args, d):
             "data": "synthetic (seeded channel draw, Poisson-Boltzmann start)",
             "config": {"workload": args.workload, "channels": count, "nodes": total_nodes,
                        "nodes_rank0": nn,
-                       "storage": args.storage + "-shifted", "tile_width": chosen,
-                       "autotune_ms_per_step": tune_ms, "cycle": 200, "graph": True,
+                       "storage": args.storage + "-shifted",
+                       "block_shape": dict(zip(("threads", "tile_width", "blocks_per_sm"), Batch.shapes()[chosen])),
+                       "autotune_ms_per_step": {"x".join(map(str, sh)): round(m, 4)
+                                                for sh, m in zip(Batch.shapes(), tune_ms)},
+                       "cycle": 200, "graph": graph,
                        "parallelism": f"channel shards x{d.world} (balanced by node count)",
                        "l2": "working set > 126 MB L2, no flush"},
             "gpu_launches": launches,

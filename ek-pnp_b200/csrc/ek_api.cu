@@ -1,8 +1,7 @@
 // ek_api.cu -- the C ABI of libekpnp (declared in include/ekpnp.h).
 //
 // Host-side owner of a channel: allocation, parameter checks, the step loop
-// (one fused LBM launch + three Poisson passes per step, the column pass of
-// the FP32 Poisson form as two kernels on two streams) and field I/O.
+// (one fused LBM launch + three Poisson passes per step) and field I/O.
 // Replaces the host code of main.cu:28-307 and the host wrappers of LBM.cu /
 // poisson.cu; every failure is returned as a status instead of exit().
 #include <cuda.h>
@@ -105,9 +104,6 @@ void free_ctx(ek_ctx *c) {
     }
     for (auto &m : c->marks)
         if (m) cudaEventDestroy(m);
-    if (c->fork) cudaEventDestroy(c->fork);
-    if (c->join) cudaEventDestroy(c->join);
-    if (c->side) cudaStreamDestroy(c->side);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -301,15 +297,6 @@ int timed(ek_ctx *c, int phase, const char *what, Fn fn, int kernels = 1) {
     return EK_OK;
 }
 
-// Side stream and fork/join events of the split column solve, made on first use.
-int side_stream(ek_ctx *c) {
-    if (c->side) return EK_OK;
-    EK_CUDA(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming), "event create");
-    EK_CUDA(cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming), "event create");
-    EK_CUDA(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking), "stream create");
-    return EK_OK;
-}
-
 // The Poisson solve of a step (or of a solve outside the step when
 // from_moments: the right-hand side from the c+, c- moments).  FP64 storage:
 // the FP64 passes on the FP64 planes.  Shifted storage, FP32 form: the passes
@@ -320,10 +307,6 @@ int poisson_now(ek_ctx *c, bool write_f64, bool from_moments = false) {
     const bool sh = shifted(c);
     const bool f32 = ek::ctx_poisson_f32(c);
     if (c->p.flags & EK_FLAG_EXPLICIT_E) write_f64 = true;  // the E planes follow psi every step
-    if (f32) {
-        int rc = side_stream(c);
-        if (rc != EK_OK) return rc;
-    }
     double *rhs = c->fields + F_RHS * c->plane, *psi = c->fields + F_PSI * c->plane;
     if (from_moments) {
         if (f32) EK_CUDA(launch_rhsf_from_moments(c->pp, c->chan, c->fields, c->stream), "rhs kernel");
@@ -334,17 +317,12 @@ int poisson_now(ek_ctx *c, bool write_f64, bool from_moments = false) {
         ++c->launches;
     }
     for (int pass = 0; pass < 3; ++pass) {
-        // FP32 form, pass B: FP64 zero mode on the side stream beside the
-        // FP32 modes (two kernels)
-        const bool split = f32 && pass == 1;
-        int rc = timed(
-            c, 1 + pass, "poisson kernel",
-            [&] {
-                if (split) return poisson_tridiag_f32_split(c->pp, c->stream, c->side, c->fork, c->join);
-                return f32 ? poisson_pass_f32(pass, c->pp, c->chan, psi, write_f64, c->stream)
-                           : poisson_pass_f64(pass, c->pp, c->chan, c->fields, c->stream);
-            },
-            split ? 2 : 1);
+        int rc = timed(c, 1 + pass, "poisson kernel", [&] {
+            // FP32 form, pass B: the FP64 zero mode rides in the FP32 modes' kernel
+            if (f32 && pass == 1) return poisson_tridiag_f32(c->pp, c->stream);
+            return f32 ? poisson_pass_f32(pass, c->pp, c->chan, psi, write_f64, c->stream)
+                       : poisson_pass_f64(pass, c->pp, c->chan, c->fields, c->stream);
+        });
         if (rc != EK_OK) return rc;
     }
     if (sh && !f32) {

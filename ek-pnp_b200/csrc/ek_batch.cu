@@ -3,23 +3,23 @@
 //
 // Each channel keeps its own context (ek_ctx: populations, fields, Poisson
 // plan, wall profiles, reference rows) and all of them step in lockstep with
-// four launches per step (five with the FP32 Poisson form, whose column solve
-// runs the FP64 zero modes on a side stream), whatever the number of channels:
+// four launches per step, whatever the number of channels:
 //   LBM      one persistent kernel over a host-built tile work-list.  A tile is
 //            {channel, first row, first column, width}; channels narrower
-//            than the block put several rows into one tile.  Every block walks
-//            a contiguous slice of the list (one wave: the grid is the number
-//            of blocks that fit on the GPU) and stages the current channel's
+//            than the block put several rows into one tile.  Blocks claim
+//            runs of tiles from a queue (one wave: the grid is the number of
+//            blocks that fit on the GPU) and stage the current channel's
 //            constants in shared memory when the channel changes.
 //   Poisson  the batched passes of ek_poisson.cu: each block's item names its
 //            channel and its first row pair (row FFTs) or first x-mode
-//            (column solve).
+//            (column solve; a channel's FP64 zero mode is an item of its own).
 // Steps run in cycles of an even number R of steps.  The last step of a cycle
 // writes the moments and, with re-basing on, the cycle ends with the re-basing
 // of every channel's shifted populations to its new row means (three more
 // launches, done in place so that device pointers never change).  A whole
-// cycle is captured once in a CUDA graph and replayed.  The block width of the
-// LBM tiles is picked by timing the candidates (ek_batch_autotune).
+// cycle is captured once in a CUDA graph and replayed.  The block shape of the
+// LBM kernel (threads, tile width, blocks per SM) is picked by timing the
+// candidates (ek_batch_autotune).
 //
 // Per step and channel the arithmetic is that of ek_step: the node update is
 // the same device function (ek_lbm_f32.cuh), the Poisson passes the same
@@ -45,11 +45,8 @@ constexpr int REFS_TPB = 256;
 // ---- kernels ---------------------------------------------------------------
 
 // Persistent LBM kernel over the tile list; TXB threads = tile width x rows.
-// Threads per SM the register allocation must allow (896: the single-channel
-// kernel's 7 blocks of 128 threads, 72 registers).
-#ifndef EK_BATCH_SM_THREADS
-#define EK_BATCH_SM_THREADS 896
-#endif
+// MINB: blocks per SM the register allocation must allow (the block shapes,
+// kShapes below, pair a width with it).
 // Tiles are handed out from a queue, TILE_CHUNK consecutive tiles (same
 // channel, adjacent rows) at a time: queue[0] is the next unclaimed tile,
 // queue[1] counts the blocks that found the list empty; the last of them
@@ -58,8 +55,8 @@ constexpr int REFS_TPB = 256;
 // replays.
 constexpr int TILE_CHUNK = 4;
 
-template <typename S, bool FIRST, bool EE, int TXB>
-__global__ void __launch_bounds__(TXB, (EK_BATCH_SM_THREADS / TXB) > 0 ? (EK_BATCH_SM_THREADS / TXB) : 1)
+template <typename S, bool FIRST, bool EE, int TXB, int MINB>
+__global__ void __launch_bounds__(TXB, MINB)
 batch_lbm(const ChanF *__restrict__ chans, const S *const *__restrict__ src, S *const *__restrict__ dst,
           double *const *__restrict__ fields, const int4 *__restrict__ tiles, int ntiles, int *__restrict__ queue,
           bool mom, int sbuf) {
@@ -82,7 +79,7 @@ batch_lbm(const ChanF *__restrict__ chans, const S *const *__restrict__ src, S *
             }
             const int r = threadIdx.x / tl.w;
             const int x = tl.z + (threadIdx.x - r * tl.w), y = tl.y + r;
-            if (x < ks.nx && y < ks.ny)
+            if (r < TXB / tl.w && x < ks.nx && y < ks.ny)
                 node_shifted<S, FIRST, EE>(ks, src[cur], dst[cur], fields[cur], x, y, mom, sbuf);
         }
         __syncthreads();  // every thread has read `claim` before thread 0 claims again
@@ -116,7 +113,7 @@ batch_rebase(const ChanF *__restrict__ chans, S *const *__restrict__ pops, float
     const ChanF &k = chans[tl.x];
     const int r = threadIdx.x / tl.w;
     const int x = tl.z + (threadIdx.x - r * tl.w), y = tl.y + r;
-    if (x >= k.nx || y >= k.ny) return;
+    if (r >= TXB / tl.w || x >= k.nx || y >= k.ny) return;  // each node of the tile once
     S *base = pops[tl.x] + (size_t)y * k.nxp + x;
     for (int pl = 0; pl < 27; ++pl) rebase_dev<S>(base + (size_t)pl * k.plane, pl, k.ny, y, k.kref, spare[tl.x]);
 }
@@ -135,13 +132,13 @@ __global__ void batch_commit_refs(const ChanF *__restrict__ chans, float *const 
 
 // ---- launchers --------------------------------------------------------------
 
-template <typename S, int TXB>
+template <typename S, int TXB, int MINB>
 cudaError_t lbm_t(const ChanF *chans, const void *src, void *dst, double *const *fields, const int4 *tiles,
                   int ntiles, int *queue, int grid, bool first, bool ee, bool mom, int sbuf, cudaStream_t s) {
     const S *const *a = (const S *const *)src;
     S *const *b = (S *const *)dst;
 #define EK_BL(F, E) \
-    batch_lbm<S, F, E, TXB><<<grid, TXB, 0, s>>>(chans, a, b, fields, tiles, ntiles, queue, mom, sbuf)
+    batch_lbm<S, F, E, TXB, MINB><<<grid, TXB, 0, s>>>(chans, a, b, fields, tiles, ntiles, queue, mom, sbuf)
     if (first) {
         if (ee) EK_BL(true, true);
         else EK_BL(true, false);
@@ -153,14 +150,34 @@ cudaError_t lbm_t(const ChanF *chans, const void *src, void *dst, double *const 
     return cudaGetLastError();
 }
 
+// Block shapes of the batched LBM kernel: threads, the widest tile (a tile is
+// min(width, nx) columns by threads / that many rows) and the blocks per SM
+// that the register allocation must allow.  At 72 registers (7 blocks of 128,
+// 14 of 64) the batched node update spills a little; 10 blocks of 64, 5 of
+// 128 and 3 of 256 do not.  Narrower tiles than threads give 2-D tiles whose
+// rows share their pulled neighbours in L1.
+struct Shape {
+    int threads, width, minb;
+};
+constexpr Shape kShapes[EK_BATCH_SHAPES] = {{64, 64, 10},   {128, 128, 5}, {128, 128, 7},
+                                             {256, 256, 3}, {256, 64, 3},  {256, 128, 3}};
+
+#define EK_SHAPE_CASES(F) F(0) F(1) F(2) F(3) F(4) F(5)
+static_assert(EK_BATCH_SHAPES == 6, "one case per shape");
+
 template <typename S>
-cudaError_t lbm_s(int txb, const ChanF *chans, const void *src, void *dst, double *const *fields, const int4 *tiles,
-                  int ntiles, int *queue, int grid, bool first, bool ee, bool mom, int sbuf, cudaStream_t s) {
-    if (txb == 64)
-        return lbm_t<S, 64>(chans, src, dst, fields, tiles, ntiles, queue, grid, first, ee, mom, sbuf, s);
-    if (txb == 256)
-        return lbm_t<S, 256>(chans, src, dst, fields, tiles, ntiles, queue, grid, first, ee, mom, sbuf, s);
-    return lbm_t<S, 128>(chans, src, dst, fields, tiles, ntiles, queue, grid, first, ee, mom, sbuf, s);
+cudaError_t lbm_s(int shape, const ChanF *chans, const void *src, void *dst, double *const *fields,
+                  const int4 *tiles, int ntiles, int *queue, int grid, bool first, bool ee, bool mom, int sbuf,
+                  cudaStream_t s) {
+    switch (shape) {
+#define EK_CASE(I)                                                                                           \
+    case I:                                                                                                  \
+        return lbm_t<S, kShapes[I].threads, kShapes[I].minb>(chans, src, dst, fields, tiles, ntiles, queue, grid, \
+                                                             first, ee, mom, sbuf, s);
+        EK_SHAPE_CASES(EK_CASE)
+#undef EK_CASE
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 template <typename S>
@@ -173,17 +190,21 @@ cudaError_t rebase_s(int txb, const ChanF *chans, void *pops, float *const *spar
     return cudaGetLastError();
 }
 
-// Blocks of the (non-first) LBM kernel resident per SM.
+// Blocks of the (non-first) LBM kernel of a shape resident per SM.
 template <typename S>
-int lbm_occupancy(int txb) {
+int lbm_occupancy(int shape) {
     int occ = 0;
-    cudaError_t e;
-    if (txb == 64)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_lbm<S, false, false, 64>, 64, 0);
-    else if (txb == 256)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_lbm<S, false, false, 256>, 256, 0);
-    else
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_lbm<S, false, false, 128>, 128, 0);
+    cudaError_t e = cudaErrorInvalidValue;
+    switch (shape) {
+#define EK_CASE(I)                                                                                                  \
+    case I:                                                                                                         \
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(                                                          \
+            &occ, batch_lbm<S, false, false, kShapes[I].threads, kShapes[I].minb>, kShapes[I].threads, 0);          \
+        break;
+        EK_SHAPE_CASES(EK_CASE)
+#undef EK_CASE
+        default: break;
+    }
     return e == cudaSuccess && occ > 0 ? occ : 1;
 }
 
@@ -198,8 +219,6 @@ struct ek_batch {
     std::vector<int64_t> ch_steps;   // steps each channel has taken in the batch
     int storage = EK_STORE_F32;
     cudaStream_t stream = nullptr;
-    cudaStream_t side = nullptr;     // FP32 Poisson form: the FP64 zero modes run here
-    cudaEvent_t fork = nullptr, join = nullptr;
     int cur = 0;                     // population buffer holding the current state (all channels)
     bool state_pre = false;
     bool explicit_e_once = false;
@@ -221,14 +240,12 @@ struct ek_batch {
     float **d_spare = nullptr;
     int4 *d_kq = nullptr;
     int4 *d_tiles = nullptr;
-    int ntiles = 0, txb = 128, grid = 0;
+    int ntiles = 0, shape = 1, txb = 128, grid = 0;  // kShapes[shape], txb = its threads
     int *d_queue = nullptr;          // LBM tile queue: next tile, finished blocks (zero between launches)
     int2 *d_pairs = nullptr;         // Poisson row-pair items
     int npairs = 0;
     int3 *d_modes = nullptr;         // Poisson x-mode items
     int nmodes = 0;
-    int3 *d_zeros = nullptr;         // FP32 form: the FP64 zero-mode items
-    int nzeros = 0;
     int2 *d_rows = nullptr;          // {channel, row} of every row
     int nrows = 0;
     // residuals
@@ -265,7 +282,7 @@ int upload(T **dst, const std::vector<T> &v, cudaStream_t s) {
 }
 
 // LBM + three Poisson passes; the FP32 form's column solve is two kernels.
-int launches_per_step(const ek_batch *b) { return b->poisson_f32 ? 5 : 4; }
+int launches_per_step(const ek_batch *) { return 4; }
 
 void release_graph(ek_batch *b) {
     if (b->graph) cudaGraphExecDestroy(b->graph);
@@ -273,13 +290,16 @@ void release_graph(ek_batch *b) {
     b->graph_cur = -1;
 }
 
-// LBM tiles of width min(txb, nx) and txb / width rows; the grid is one wave.
-int build_tiles(ek_batch *b, int txb) {
+// LBM tiles of a block shape: min(width, nx) columns by threads / that many
+// rows; the grid is one wave.
+int build_tiles(ek_batch *b, int shape) {
+    if (shape < 0 || shape >= EK_BATCH_SHAPES) return ek::ctx_fail(EK_ERR_INVALID, "no such block shape");
+    const int txb = kShapes[shape].threads;
     std::vector<int4> tiles;
     for (size_t i = 0; i < b->ch.size(); ++i) {
         if (!b->active[i]) continue;
         const ek_params &p = b->ch[i]->p;
-        const int w = std::min(txb, p.nx);
+        const int w = std::min(kShapes[shape].width, p.nx);
         const int rows = txb / w;
         for (int y = 0; y < p.ny; y += rows)
             for (int x0 = 0; x0 < p.nx; x0 += w) tiles.push_back(make_int4((int)i, y, x0, w));
@@ -293,10 +313,11 @@ int build_tiles(ek_batch *b, int txb) {
     }
     b->ntiles = (int)tiles.size();
     b->txb = txb;
+    b->shape = shape;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int occ = b->storage == EK_STORE_F16 ? lbm_occupancy<__half>(txb) : lbm_occupancy<float>(txb);
+    const int occ = b->storage == EK_STORE_F16 ? lbm_occupancy<__half>(shape) : lbm_occupancy<float>(shape);
     b->grid = std::max(1, std::min((b->ntiles + TILE_CHUNK - 1) / TILE_CHUNK, sms * occ));
     return EK_OK;
 }
@@ -311,7 +332,7 @@ int build_tables(ek_batch *b) {
     std::vector<float *> sp;
     std::vector<int4> kq, ritems;
     std::vector<int2> pairs, rows, rranges;
-    std::vector<int3> modes, zeros;
+    std::vector<int3> modes, zeros;  // column items: zero modes first (the longer blocks start first)
     release_graph(b);
     b->kcur.clear();
     int nrpart = 0;
@@ -344,8 +365,8 @@ int build_tables(ek_batch *b) {
             const int per = 256 / (nx >> 4);
             for (int q = 0; q < (n + 1) / 2; q += per) pairs.push_back(make_int2((int)i, q));
             const int M = poisson_tridiag_modes(n);
-            // the zero mode in FP64 (modes 0..M-1 of the FP64 spectrum); modes 1.. in FP32
-            zeros.push_back(make_int3((int)i, 0, M));
+            // the zero mode in FP64 (an item with 0 modes per block); modes 1.. in FP32
+            zeros.push_back(make_int3((int)i, 0, 0));
             for (int m0 = 1; m0 <= nx / 2; m0 += M) modes.push_back(make_int3((int)i, m0, M));
             for (int y = 0; y < c->p.ny; ++y) rows.push_back(make_int2((int)i, y));
         }
@@ -365,14 +386,13 @@ int build_tables(ek_batch *b) {
     if ((rc = upload(&b->d_spare, sp, b->stream)) != EK_OK) return rc;
     if ((rc = upload(&b->d_kq, kq, b->stream)) != EK_OK) return rc;
     if ((rc = upload(&b->d_pairs, pairs, b->stream)) != EK_OK) return rc;
+    modes.insert(modes.begin(), zeros.begin(), zeros.end());
     if ((rc = upload(&b->d_modes, modes, b->stream)) != EK_OK) return rc;
-    if ((rc = upload(&b->d_zeros, zeros, b->stream)) != EK_OK) return rc;
     if ((rc = upload(&b->d_rows, rows, b->stream)) != EK_OK) return rc;
     if ((rc = upload(&b->d_ritems, ritems, b->stream)) != EK_OK) return rc;
     if ((rc = upload(&b->d_rranges, rranges, b->stream)) != EK_OK) return rc;
     b->npairs = (int)pairs.size();
     b->nmodes = (int)modes.size();
-    b->nzeros = (int)zeros.size();
     b->nrows = (int)rows.size();
     b->nritems = (int)ritems.size();
     if (b->d_rpart) cudaFree(b->d_rpart);
@@ -387,16 +407,14 @@ int launch_step(ek_batch *b, bool first, bool ee, bool mom) {
     const void *src = b->d_pops[b->cur];
     void *dst = b->d_pops[b->cur ^ 1];
     cudaError_t e = b->storage == EK_STORE_F16
-                        ? lbm_s<__half>(b->txb, b->d_chanf, src, dst, b->d_fields, b->d_tiles, b->ntiles,
+                        ? lbm_s<__half>(b->shape, b->d_chanf, src, dst, b->d_fields, b->d_tiles, b->ntiles,
                                         b->d_queue, b->grid, first, ee, mom, b->cur, b->stream)
-                        : lbm_s<float>(b->txb, b->d_chanf, src, dst, b->d_fields, b->d_tiles, b->ntiles,
+                        : lbm_s<float>(b->shape, b->d_chanf, src, dst, b->d_fields, b->d_tiles, b->ntiles,
                                        b->d_queue, b->grid, first, ee, mom, b->cur, b->stream);
     EK_BCUDA(e, "batch LBM kernel");
     EK_BCUDA(batch_poisson(0, b->d_plans, b->d_chan, b->d_fields, b->d_pairs, b->npairs, false, b->stream),
              "batch rows");
-    EK_BCUDA(batch_tridiag_f32_split(b->d_plans, b->d_zeros, b->nzeros, b->d_modes, b->nmodes, b->stream, b->side,
-                                     b->fork, b->join),
-             "batch modes");
+    EK_BCUDA(batch_tridiag_f32(b->d_plans, b->d_modes, b->nmodes, b->stream), "batch modes");
     // the FP64 psi planes follow on the steps that write the moments
     EK_BCUDA(batch_poisson(2, b->d_plans, b->d_chan, b->d_fields, b->d_pairs, b->npairs, mom, b->stream),
              "batch rows");
@@ -506,13 +524,6 @@ int ek_batch_create(const ek_params *params, int32_t count, ek_batch **out) {
         ek_batch_destroy(b);
         return cuda_err(e, "stream create");
     }
-    e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming);
-    if (e != cudaSuccess) {
-        ek_batch_destroy(b);
-        return cuda_err(e, "stream create");
-    }
     for (int32_t i = 0; i < count; ++i) {
         ek_ctx *c = nullptr;
         int rc = ek_create(&params[i], &c);
@@ -528,7 +539,7 @@ int ek_batch_create(const ek_params *params, int32_t count, ek_batch **out) {
         b->nodes += (int64_t)params[i].nx * params[i].ny;
     }
     int rc = build_tables(b);
-    if (rc == EK_OK) rc = build_tiles(b, 128);
+    if (rc == EK_OK) rc = build_tiles(b, 1);
     if (rc != EK_OK) {
         ek_batch_destroy(b);
         return rc;
@@ -544,12 +555,9 @@ int ek_batch_destroy(ek_batch *b) {
     for (ek_ctx *c : b->ch) ek_destroy(c);  // the channels do not own the batch's stream
     void *tables[] = {b->d_chanf, b->d_chan,  b->d_plans,  b->d_pops[0],  b->d_pops[1], b->d_fields,
                       b->d_spare, b->d_kq,    b->d_tiles,  b->d_pairs,    b->d_modes,   b->d_rows,
-                      b->d_snaps, b->d_ritems, b->d_rranges, b->d_rpart,  b->d_zeros, b->d_queue};
+                      b->d_snaps, b->d_ritems, b->d_rranges, b->d_rpart,  b->d_queue};
     for (void *t : tables)
         if (t) cudaFree(t);
-    if (b->fork) cudaEventDestroy(b->fork);
-    if (b->join) cudaEventDestroy(b->join);
-    if (b->side) cudaStreamDestroy(b->side);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return EK_OK;
@@ -601,7 +609,7 @@ int ek_batch_init_equilibrium(ek_batch *b) {
     b->explicit_e_once = ee;
     b->steps = 0;
     int rc = build_tables(b);  // reference buffers may have changed
-    if (rc == EK_OK) rc = build_tiles(b, b->txb);
+    if (rc == EK_OK) rc = build_tiles(b, b->shape);
     if (rc != EK_OK) return rc;
     EK_BCUDA(cudaStreamSynchronize(b->stream), "batch init");
     sync_channel_state(b, 0);
@@ -661,17 +669,24 @@ int ek_batch_launch_count(const ek_batch *b, int64_t *out) {
     return EK_OK;
 }
 
-int ek_batch_tile_width(const ek_batch *b, int32_t *out) {
-    if (!b || !out) return ek::ctx_fail(EK_ERR_INVALID, "null argument");
-    *out = b->txb;
+int ek_batch_shape_info(int32_t index, int32_t *threads, int32_t *width, int32_t *blocks_per_sm) {
+    if (index < 0 || index >= EK_BATCH_SHAPES) return ek::ctx_fail(EK_ERR_INVALID, "no such block shape");
+    if (threads) *threads = kShapes[index].threads;
+    if (width) *width = kShapes[index].width;
+    if (blocks_per_sm) *blocks_per_sm = kShapes[index].minb;
     return EK_OK;
 }
 
-int ek_batch_set_tile_width(ek_batch *b, int32_t width) {
-    if (!b || (width != 64 && width != 128 && width != 256))
-        return ek::ctx_fail(EK_ERR_INVALID, "tile width must be 64, 128 or 256");
+int ek_batch_shape(const ek_batch *b, int32_t *out) {
+    if (!b || !out) return ek::ctx_fail(EK_ERR_INVALID, "null argument");
+    *out = b->shape;
+    return EK_OK;
+}
+
+int ek_batch_set_shape(ek_batch *b, int32_t index) {
+    if (!b || index < 0 || index >= EK_BATCH_SHAPES) return ek::ctx_fail(EK_ERR_INVALID, "no such block shape");
     EK_BCUDA(cudaStreamSynchronize(b->stream), "batch sync");
-    return build_tiles(b, width);
+    return build_tiles(b, index);
 }
 
 int ek_batch_stream(const ek_batch *b, void **out) {
@@ -697,7 +712,7 @@ int ek_batch_resync(ek_batch *b) {
     b->explicit_e_once = c0->explicit_e_once;
     for (size_t i = 0; i < b->ch.size(); ++i) b->ch_steps[i] = b->ch[i]->steps;
     int rc = build_tables(b);  // reference rows and exponents may have changed
-    if (rc == EK_OK) rc = build_tiles(b, b->txb);
+    if (rc == EK_OK) rc = build_tiles(b, b->shape);
     return rc;
 }
 
@@ -720,7 +735,7 @@ int ek_batch_set_active(ek_batch *b, const uint8_t *mask) {
     }
     if (!changed) return EK_OK;
     int rc = build_tables(b);
-    if (rc == EK_OK) rc = build_tiles(b, b->txb);
+    if (rc == EK_OK) rc = build_tiles(b, b->shape);
     return rc;
 }
 
@@ -768,23 +783,22 @@ int ek_batch_residual(ek_batch *b, int32_t interval, double *out5, double *worst
     return EK_OK;
 }
 
-// Time each tile width for `steps` steps (the state advances by 3 (steps + 2)
-// steps) and keep the fastest; ms3 (optional) gets the ms per step of 64, 128
-// and 256.
-int ek_batch_autotune(ek_batch *b, int32_t steps, int32_t *chosen, double *ms3) {
+// Time each block shape for `steps` steps (the state advances by
+// EK_BATCH_SHAPES (steps + 2) steps) and keep the fastest; ms (optional) gets
+// the ms per step of every shape.
+int ek_batch_autotune(ek_batch *b, int32_t steps, int32_t *chosen, double *ms) {
     if (!b || steps <= 0) return ek::ctx_fail(EK_ERR_INVALID, "bad autotune arguments");
     int rc = check_channels(b);
     if (rc != EK_OK) return rc;
-    const int cand[3] = {64, 128, 256};
     double best = 1e300;
-    int best_w = b->txb;
+    int best_w = b->shape;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     EK_BCUDA(cudaEventCreate(&e0), "event");
     EK_BCUDA(cudaEventCreate(&e1), "event");
     const bool saved_graph = b->use_graph;
     b->use_graph = false;  // time the kernels, not a graph captured for one width
-    for (int k = 0; k < 3 && rc == EK_OK; ++k) {
-        rc = build_tiles(b, cand[k]);
+    for (int k = 0; k < EK_BATCH_SHAPES && rc == EK_OK; ++k) {
+        rc = build_tiles(b, k);
         if (rc == EK_OK) rc = ek_batch_step(b, 2);  // warm-up
         if (rc != EK_OK) break;
         cudaEventRecord(e0, b->stream);
@@ -796,13 +810,13 @@ int ek_batch_autotune(ek_batch *b, int32_t steps, int32_t *chosen, double *ms3) 
             rc = cuda_err(e, "autotune");
             break;
         }
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        const double per = ms / steps;
-        if (ms3) ms3[k] = per;
+        float elapsed = 0.0f;
+        cudaEventElapsedTime(&elapsed, e0, e1);
+        const double per = elapsed / steps;
+        if (ms) ms[k] = per;
         if (per < best) {
             best = per;
-            best_w = cand[k];
+            best_w = k;
         }
     }
     cudaEventDestroy(e0);

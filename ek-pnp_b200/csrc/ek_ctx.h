@@ -14,8 +14,6 @@ struct ek_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
-    cudaStream_t side = nullptr;          // FP32 Poisson form: the FP64 zero mode runs here
-    cudaEvent_t fork = nullptr, join = nullptr;
     int nxp = 0, mp = 0, n = 0;
     size_t plane = 0;
     void *pops[2] = {nullptr, nullptr};

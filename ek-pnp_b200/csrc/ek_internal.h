@@ -222,7 +222,7 @@ size_t poisson_smem_bytes_f64(int nx);
 // fluctuation about each row's mean; the row sums (the zero mode), its
 // column solve and the mean of psi in FP64.
 bool poisson_f32_supported(const PoissonPlan &pp);
-// Passes 0 and 2 (pass 1 is poisson_tridiag_f32_split): pass 0 reads
+// Passes 0 and 2 (pass 1 is poisson_tridiag_f32): pass 0 reads
 // pp.rhsf with the row constants of c.kref and the wall lifting; pass 2 writes
 // pp.psif and pp.psim, and the FP64 psi plane too when write_f64.
 cudaError_t poisson_pass_f32(int pass, const PoissonPlan &pp, const Chan &c, double *psi, bool write_f64,
@@ -244,16 +244,15 @@ __host__ __device__ inline double rhs_row_constant(const PoissonPlan &pp, const 
 cudaError_t launch_split_psi(const PoissonPlan &pp, const Chan &c, const double *psi, cudaStream_t s);
 // rhsf from the c+, c- moments (a solve outside the step, FP32 form).
 cudaError_t launch_rhsf_from_moments(const PoissonPlan &pp, const Chan &c, const double *fields, cudaStream_t s);
-// Pass B of the FP32 form as two kernels on two streams: the FP64 zero mode
-// on `side`, the FP32 modes on `s` (fork/join through the two events).
-cudaError_t poisson_tridiag_f32_split(const PoissonPlan &pp, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
-                                      cudaEvent_t join);
-cudaError_t batch_tridiag_f32_split(const PoissonPlan *plans, const void *zero_items, int nzero, const void *mode_items,
-                                    int nmodes, cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join);
+// Pass B of the FP32 form, one kernel: the FP64 zero mode in its first
+// block, the FP32 modes in the others.  Batched: items int3 {channel, first
+// mode, modes per block}, modes per block 0 naming a channel's zero mode.
+cudaError_t poisson_tridiag_f32(const PoissonPlan &pp, cudaStream_t s);
+cudaError_t batch_tridiag_f32(const PoissonPlan *plans, const void *items, int nitems, cudaStream_t s);
 // Batched Poisson passes of the FP32 form over many channels (ek_batch.cu
 // builds the items): pass 0/2 items int2 {channel, first row pair}
 // (256-thread blocks, each 256/(nx/16) row pairs; power-of-two nx from 16 to
-// 4096); pass 1 is batch_tridiag_f32_split.  write_f64 as poisson_pass_f32.
+// 4096); pass 1 is batch_tridiag_f32.  write_f64 as poisson_pass_f32.
 cudaError_t batch_poisson(int pass, const PoissonPlan *plans, const Chan *chans, double *const *fields,
                           const void *items, int nitems, bool write_f64, cudaStream_t s);
 int poisson_tridiag_modes(int n);

@@ -734,33 +734,105 @@ __global__ void __launch_bounds__(TB_THREADS) tridiag_part(const PoissonPlan pp,
     tridiag_part_dev(pp, M, blockIdx.x * M, sh);
 }
 
-// FP32 form of pass B as two kernels that the caller runs on two streams:
-// the zero mode in FP64 (the FP64 spectrum's column 0, with its neighbours
-// up to M-1 solved alongside and unused) in one block without a register
-// cap, and modes 1..nx/2 in FP32, M per block, two blocks per SM.
-__global__ void __launch_bounds__(TB_THREADS) tridiag_zero_f64(const PoissonPlan pp, int M) {
-    __shared__ TridiagShared sh;
-    tridiag_part_dev(pp, M, 0, sh);
+// Shared memory of the FP32 form's column kernel: the FP32 modes' segment
+// ends, or the FP64 zero mode's (real) affine maps.
+union ColumnShared {
+    TridiagSharedT<float, float2> f;
+    struct {
+        double e[TB_THREADS];
+        double f[TB_THREADS];
+    } z;
+};
+
+// Value entering this thread's segment of the zero mode: the real affine maps
+// D -> e + f D of the block's TB_THREADS segments composed in order (forward
+// from segment 0 or backward from the last), log2(TB_THREADS) rounds.
+template <bool FWD>
+__device__ __forceinline__ double zero_carry(double e, double f, ColumnShared &sh) {
+    const int t = threadIdx.x;
+    for (int off = 1; off < TB_THREADS; off <<= 1) {
+        sh.z.e[t] = e;
+        sh.z.f[t] = f;
+        __syncthreads();
+        const int src = FWD ? t - off : t + off;
+        if (FWD ? src >= 0 : src < TB_THREADS) {
+            e = e + f * sh.z.e[src];
+            f = f * sh.z.f[src];
+        }
+        __syncthreads();
+    }
+    sh.z.e[t] = e;
+    __syncthreads();
+    const int prev = FWD ? t - 1 : t + 1;
+    const double out = (FWD ? prev >= 0 : prev < TB_THREADS) ? sh.z.e[prev] : 0.0;
+    __syncthreads();
+    return out;
 }
 
+// The zero mode (kx = 0) of the FP32 form's column solve in FP64, by one
+// block: thread t owns rows [t L, t L + L) of column 0 of the FP64 spectrum
+// (the row sums, real), L = ceil(n / TB_THREADS).  The partitioned Thomas
+// solve of tridiag_part_gen with the channel's FP64 pivots, but working on
+// the column in place (L2-resident, 8 n bytes) rather than in registers, so
+// that it fits the FP32 kernel's register budget.
+__device__ __forceinline__ void zero_mode_f64(const PoissonPlan &pp, ColumnShared &sh) {
+    const int n = pp.n, L = (n + TB_THREADS - 1) / TB_THREADS;
+    const int ja = (int)threadIdx.x * L, cnt = max(0, min(n, ja + L) - ja);
+    const size_t mp = (size_t)pp.mp;
+    double *col = &pp.spec[0].x;  // element j at col[2 j mp]
+    const double *piv = pp.piv;
+    const double dy2 = pp.dy2;
+    // forward sweep of the segment from a zero entry value
+    double d = 0.0, mu = 1.0;
+    for (int q = 0; q < cnt; ++q) {
+        const size_t j = (size_t)(ja + q) * mp;
+        const double c = piv[j];
+        d = (dy2 * col[2 * j] - d) * c;
+        mu = -c * mu;
+        col[2 * j] = d;
+    }
+    const double D = zero_carry<true>(d, mu, sh);
+    // true forward values, then the backward sweep from a zero exit value
+    mu = 1.0;
+    for (int q = 0; q < cnt; ++q) {
+        const size_t j = (size_t)(ja + q) * mp;
+        mu = -piv[j] * mu;
+        col[2 * j] += mu * D;
+    }
+    double x = 0.0, nu = 1.0;
+    for (int q = cnt - 1; q >= 0; --q) {
+        const size_t j = (size_t)(ja + q) * mp;
+        const double c = piv[j];
+        x = col[2 * j] - c * x;
+        nu = -c * nu;
+        col[2 * j] = x;
+    }
+    const double X = zero_carry<false>(x, nu, sh);
+    nu = 1.0;
+    for (int q = cnt - 1; q >= 0; --q) {
+        const size_t j = (size_t)(ja + q) * mp;
+        nu = -piv[j] * nu;
+        col[2 * j] += nu * X;
+    }
+}
+
+// Pass B of the FP32 form in one kernel: block 0 solves the zero mode in
+// FP64 (zero_mode_f64), blocks 1.. the modes 1..nx/2 in FP32, M per block,
+// two blocks per SM.
 __global__ void __launch_bounds__(TB_THREADS, 2) tridiag_modes_f32(const PoissonPlan pp, int M) {
-    __shared__ TridiagSharedT<float, float2> sh;
+    __shared__ ColumnShared sh;
+    if (blockIdx.x == 0) {
+        zero_mode_f64(pp, sh);
+        return;
+    }
     tridiag_part_gen<float, float2>(pp.pivf, pp.specf, pp.n, pp.nx, (size_t)pp.mp, (float)pp.dy2, M,
-                                    1 + blockIdx.x * M, sh);
+                                    1 + (blockIdx.x - 1) * M, sh.f);
 }
 
 // ---- batched passes: one launch for many channels -------------------------
 // A block's work item names its channel and its first row pair (passes A,
 // C) or first x-mode (pass B); the channel's plan comes from a device table.
-// Batches run the FP32 form; the zero modes' FP64 column solve is batch_tridiag.
-__global__ void __launch_bounds__(TB_THREADS)
-batch_tridiag(const PoissonPlan *__restrict__ plans, const int3 *__restrict__ items) {
-    __shared__ TridiagShared sh;
-    const int3 it = items[blockIdx.x];
-    const PoissonPlan pp = plans[it.x];
-    tridiag_part_dev(pp, it.z, it.y, sh);
-}
-
+// Batches run the FP32 form.
 __global__ void __launch_bounds__(256, 4)
 batch_fwd_rows_f32(const PoissonPlan *__restrict__ plans, const Chan *__restrict__ chans,
                    const int2 *__restrict__ items) {
@@ -781,14 +853,19 @@ batch_inv_rows_f32(const PoissonPlan *__restrict__ plans, const Chan *__restrict
     inv_rows_r16f_dev<256>(pp, c, fields[it.x] + F_PSI * c.plane, write_f64, it.y, (float2 *)smraw);
 }
 
-// items {channel, first mode, modes per block}: FP32 mode blocks (the zero
-// mode runs in batch_tridiag, FP64)
+// items {channel, first mode, modes per block}: FP32 mode blocks, and for
+// modes per block == 0 the channel's FP64 zero mode (zero_mode_f64)
 __global__ void __launch_bounds__(TB_THREADS, 2)
 batch_tridiag_modes_f32(const PoissonPlan *__restrict__ plans, const int3 *__restrict__ items) {
-    __shared__ TridiagSharedT<float, float2> sh;
+    __shared__ ColumnShared sh;
     const int3 it = items[blockIdx.x];
     const PoissonPlan pp = plans[it.x];
-    tridiag_part_gen<float, float2>(pp.pivf, pp.specf, pp.n, pp.nx, (size_t)pp.mp, (float)pp.dy2, it.z, it.y, sh);
+    if (it.z == 0) {
+        zero_mode_f64(pp, sh);
+        return;
+    }
+    tridiag_part_gen<float, float2>(pp.pivf, pp.specf, pp.n, pp.nx, (size_t)pp.mp, (float)pp.dy2, it.z, it.y,
+                                    sh.f);
 }
 
 // Modes per block of tridiag_part for n rows, so that every segment has at
@@ -856,24 +933,16 @@ bool poisson_f32_supported(const PoissonPlan &pp) {
     return use_r16(pp) && tridiag_modes(pp.n) > 0 && pp.twf && pp.pivf && pp.specf && pp.rowmean && pp.rowmean_ok;
 }
 
-cudaError_t poisson_tridiag_f32_split(const PoissonPlan &pp, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
-                                      cudaEvent_t join) {
+cudaError_t poisson_tridiag_f32(const PoissonPlan &pp, cudaStream_t s) {
     if (!poisson_f32_supported(pp)) return cudaErrorInvalidValue;
     const int M = tridiag_modes(pp.n);
-    cudaError_t e = cudaEventRecord(fork, s);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(side, fork, 0);
-    if (e != cudaSuccess) return e;
-    tridiag_zero_f64<<<1, TB_THREADS, 0, side>>>(pp, M);
-    tridiag_modes_f32<<<(pp.nx / 2 + M - 1) / M, TB_THREADS, 0, s>>>(pp, M);
-    e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaEventRecord(join, side);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, join, 0);
-    return e;
+    tridiag_modes_f32<<<1 + (pp.nx / 2 + M - 1) / M, TB_THREADS, 0, s>>>(pp, M);
+    return cudaGetLastError();
 }
 
 cudaError_t poisson_pass_f32(int pass, const PoissonPlan &pp, const Chan &c, double *psi, bool write_f64,
                              cudaStream_t s) {
-    // pass B of this form runs through poisson_tridiag_f32_split
+    // pass B of this form runs through poisson_tridiag_f32
     if (!poisson_f32_supported(pp) || pass == 1) return cudaErrorInvalidValue;
     int threads, per;
     r16_shape(pp.nx, &threads, &per);
@@ -892,7 +961,7 @@ cudaError_t poisson_pass_f32(int pass, const PoissonPlan &pp, const Chan &c, dou
 cudaError_t batch_poisson(int pass, const PoissonPlan *plans, const Chan *chans, double *const *fields,
                           const void *items, int nitems, bool write_f64, cudaStream_t s) {
     if (nitems <= 0) return cudaSuccess;
-    if (pass == 1) return cudaErrorInvalidValue;  // runs through batch_tridiag_f32_split
+    if (pass == 1) return cudaErrorInvalidValue;  // runs through batch_tridiag_f32
     if (pass == 0)
         batch_fwd_rows_f32<<<nitems, 256, 32768, s>>>(plans, chans, (const int2 *)items);
     else
@@ -900,17 +969,9 @@ cudaError_t batch_poisson(int pass, const PoissonPlan *plans, const Chan *chans,
     return cudaGetLastError();
 }
 
-cudaError_t batch_tridiag_f32_split(const PoissonPlan *plans, const void *zero_items, int nzero, const void *mode_items,
-                                    int nmodes, cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join) {
-    cudaError_t e = cudaEventRecord(fork, s);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(side, fork, 0);
-    if (e != cudaSuccess) return e;
-    if (nzero > 0) batch_tridiag<<<nzero, TB_THREADS, 0, side>>>(plans, (const int3 *)zero_items);
-    if (nmodes > 0) batch_tridiag_modes_f32<<<nmodes, TB_THREADS, 0, s>>>(plans, (const int3 *)mode_items);
-    e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaEventRecord(join, side);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, join, 0);
-    return e;
+cudaError_t batch_tridiag_f32(const PoissonPlan *plans, const void *items, int nitems, cudaStream_t s) {
+    if (nitems > 0) batch_tridiag_modes_f32<<<nitems, TB_THREADS, 0, s>>>(plans, (const int3 *)items);
+    return cudaGetLastError();
 }
 
 cudaError_t poisson_set_smem_limits() {

@@ -104,8 +104,10 @@ _SIGS = {
     "ek_batch_sync": ([ctypes.c_void_p], ctypes.c_int),
     "ek_batch_step_count": ([ctypes.c_void_p, _P(ctypes.c_int64)], ctypes.c_int),
     "ek_batch_launch_count": ([ctypes.c_void_p, _P(ctypes.c_int64)], ctypes.c_int),
-    "ek_batch_tile_width": ([ctypes.c_void_p, _P(ctypes.c_int32)], ctypes.c_int),
-    "ek_batch_set_tile_width": ([ctypes.c_void_p, ctypes.c_int32], ctypes.c_int),
+    "ek_batch_shape_info": ([ctypes.c_int32, _P(ctypes.c_int32), _P(ctypes.c_int32), _P(ctypes.c_int32)],
+                            ctypes.c_int),
+    "ek_batch_shape": ([ctypes.c_void_p, _P(ctypes.c_int32)], ctypes.c_int),
+    "ek_batch_set_shape": ([ctypes.c_void_p, ctypes.c_int32], ctypes.c_int),
     "ek_batch_autotune": ([ctypes.c_void_p, ctypes.c_int32, _P(ctypes.c_int32), _dp], ctypes.c_int),
     "ek_batch_residual": ([ctypes.c_void_p, ctypes.c_int32, _dp, _dp], ctypes.c_int),
     "ek_batch_set_active": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),

@@ -91,23 +91,35 @@ class Batch:
         check(lib().ek_batch_stream(self._h, ctypes.byref(v)))
         return int(v.value or 0)
 
+    @staticmethod
+    def shapes():
+        """Block shapes of the batched LBM kernel: (threads, widest tile, blocks per SM)."""
+        out = []
+        n = 0
+        while True:
+            t, w, m = ctypes.c_int32(0), ctypes.c_int32(0), ctypes.c_int32(0)
+            if lib().ek_batch_shape_info(n, ctypes.byref(t), ctypes.byref(w), ctypes.byref(m)) != 0:
+                return out
+            out.append((int(t.value), int(w.value), int(m.value)))
+            n += 1
+
     @property
-    def tile_width(self):
+    def shape(self):
         v = ctypes.c_int32(0)
-        check(lib().ek_batch_tile_width(self._h, ctypes.byref(v)))
+        check(lib().ek_batch_shape(self._h, ctypes.byref(v)))
         return int(v.value)
 
-    @tile_width.setter
-    def tile_width(self, w):
-        check(lib().ek_batch_set_tile_width(self._h, int(w)))
+    @shape.setter
+    def shape(self, index):
+        check(lib().ek_batch_set_shape(self._h, int(index)))
 
     def autotune(self, steps=20):
-        """Time each tile width (advances the state); returns (chosen, {width: ms/step})."""
+        """Time each block shape (advances the state); returns (chosen index, [ms/step per shape])."""
         chosen = ctypes.c_int32(0)
-        ms = np.zeros(3)
+        ms = np.zeros(len(self.shapes()))
         check(lib().ek_batch_autotune(self._h, int(steps), ctypes.byref(chosen),
                                       ms.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
-        return int(chosen.value), dict(zip((64, 128, 256), ms.tolist()))
+        return int(chosen.value), ms.tolist()
 
     def resync(self):
         """Adopt the channels' current states (after Channel.tile_x)."""

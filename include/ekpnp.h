@@ -327,9 +327,8 @@ int ek_diag_umax(int32_t nx, int32_t ny, const double *uy, double *out);
 /* ---- batches of independent channels ------------------------------------
  * No counterpart in the reference (one channel per run of main.cu).  A batch
  * steps many channels of different sizes and parameters in lockstep, four
- * kernel launches per step for all of them (five with the FP32 Poisson form):
- * one persistent LBM kernel over a tile work-list and three batched Poisson
- * passes, the FP32 form's column pass as two kernels on two streams.  Each channel is an ek_ctx
+ * kernel launches per step for all of them: one persistent LBM kernel over a
+ * tile work-list and three batched Poisson passes.  Each channel is an ek_ctx
  * owned by the batch (ek_batch_channel); use it for ek_set_fields,
  * ek_set_wall_profile, ek_init_poisson_boltzmann, ek_get_fields and
  * ek_residual, but step it only through the batch.  Per channel, a batch step
@@ -356,14 +355,18 @@ int ek_batch_step(ek_batch *b, int32_t nsteps);
 int ek_batch_sync(ek_batch *b);
 int ek_batch_step_count(const ek_batch *b, int64_t *out);
 int ek_batch_launch_count(const ek_batch *b, int64_t *out);
-/* Threads per LBM block (64, 128 or 256): tile width min(width, nx), and
- * width / min(width, nx) rows per tile. */
-int ek_batch_tile_width(const ek_batch *b, int32_t *width);
-int ek_batch_set_tile_width(ek_batch *b, int32_t width);
-/* Times `steps` steps at each tile width (the state advances by
- * 3 (steps + 2) steps), keeps the fastest; ms3 (optional): ms per step of
- * widths 64, 128, 256. */
-int ek_batch_autotune(ek_batch *b, int32_t steps, int32_t *chosen, double *ms3);
+/* Block shapes of the batched LBM kernel, indices 0 .. EK_BATCH_SHAPES-1:
+ * threads per block, the widest tile (a tile is min(width, nx) columns by
+ * threads / min(width, nx) rows) and the blocks per SM that the kernel's
+ * register allocation allows.  Every shape gives the same bits. */
+#define EK_BATCH_SHAPES 6
+int ek_batch_shape_info(int32_t index, int32_t *threads, int32_t *width, int32_t *blocks_per_sm);
+int ek_batch_shape(const ek_batch *b, int32_t *index);
+int ek_batch_set_shape(ek_batch *b, int32_t index);
+/* Times `steps` steps in each block shape (the state advances by
+ * EK_BATCH_SHAPES (steps + 2) steps) and keeps the fastest; chosen: its
+ * index; ms (optional, EK_BATCH_SHAPES values): ms per step of each shape. */
+int ek_batch_autotune(ek_batch *b, int32_t steps, int32_t *chosen, double *ms);
 /* Freeze (mask[i] == 0) or step (mask[i] != 0) each channel; a frozen
  * channel keeps its state and step count, the launches per step stay the
  * same and the work shrinks to the active channels (a run to steady state freezes

@@ -70,8 +70,8 @@ def test_launch_accounting_and_profile():
             ch.profile(True)
             ch.step(25)
             prof = ch.profile_read()
-            # the FP32 Poisson form (shifted storage) solves its columns in two kernels
-            per_step = 4 if storage == ekpnp.STORE_F64 else 5
+            # one LBM kernel and three Poisson passes, in every storage form
+            per_step = 4
             assert ch.launches - n0 == per_step * 25
             assert all(prof[ph][1] == 25 for ph in ch.PHASES)
             assert all(prof[ph][0] > 0 for ph in ch.PHASES)

@@ -59,15 +59,15 @@ def singles(storage):
     return {steps: [single(p, i, steps, 10) for p, i in zip(ps, ins)] for steps in (37,)}
 
 
-@pytest.mark.parametrize("width", [64, 128, 256])
+@pytest.mark.parametrize("shape", range(6))
 @pytest.mark.parametrize("graph", [True, False])
-def test_batch_bitwise_equals_single_channels(storage, singles, width, graph):
+def test_batch_bitwise_equals_single_channels(storage, singles, shape, graph):
     import ekpnp
     with ekpnp.Batch(params(storage)) as b:
         for ch, init in zip(b, inits()):
             ch.set_fields(**init)
         b.set_cycle(10, rebase=True, graph=graph)
-        b.tile_width = width
+        b.shape = shape
         b.init_equilibrium()
         b.step(5)       # first step + partial cycle
         b.step(30)      # cycle-aligned run: graphs of 10 steps where allowed
@@ -83,7 +83,7 @@ def test_batch_bitwise_equals_single_channels(storage, singles, width, graph):
 
 def test_autotune_keeps_the_bits():
     import ekpnp
-    steps = 3 * (4 + 2) + 11
+    steps = 6 * (4 + 2) + 11
     ref = [single(p, i, steps, 10) for p, i in zip(params(ekpnp.STORE_F32), inits())]
     with ekpnp.Batch(params(ekpnp.STORE_F32)) as b:
         for ch, init in zip(b, inits()):
@@ -91,8 +91,8 @@ def test_autotune_keeps_the_bits():
         b.set_cycle(10)
         b.init_equilibrium()
         w, ms = b.autotune(4)
-        assert w in (64, 128, 256) and b.tile_width == w
-        assert all(v > 0 for v in ms.values())
+        assert w in range(len(ekpnp.Batch.shapes())) and b.shape == w
+        assert len(ms) == len(ekpnp.Batch.shapes()) and all(v > 0 for v in ms)
         b.step(11)
         for i, ch in enumerate(b):
             got = ch.get_fields(NAMES)
@@ -136,9 +136,9 @@ def test_launch_count_is_independent_of_channel_count():
             b.step(40)
             b.sync()
             counts.append(b.launches - before)
-    # 5 launches per step (FP32 Poisson form: two column-solve kernels) + 3
-    # re-basing launches per cycle, whatever the batch size
-    assert counts[0] == counts[1] == 40 * 5 + 4 * 3
+    # 4 launches per step (the column pass carries the FP64 zero modes in its
+    # own blocks) + 3 re-basing launches per cycle, whatever the batch size
+    assert counts[0] == counts[1] == 40 * 4 + 4 * 3
 
 
 def test_stepping_a_channel_alone_is_refused():
