@@ -87,6 +87,7 @@ void free_ctx(ek_ctx *c) {
     cudaFree(c->wdelta);
     cudaFree(c->lift);
     cudaFree(c->err_dev);
+    cudaFree(c->jacobi_word);
     cudaFree(c->pp.tw);
     cudaFree(c->pp.piv);
     cudaFree(c->pp.spec);
@@ -401,6 +402,14 @@ void ctx_refresh(ek_ctx *c) { refresh_chan(c); }
 bool ctx_poisson_f32(const ek_ctx *c) {
     if (c->poisson_mode == 1 || c->p.storage == EK_STORE_F64) return false;
     return poisson_f32_supported(c->pp);
+}
+
+int ctx_after_psi(ek_ctx *c) {
+    EK_CUDA(launch_efield_f64(c->chan, c->fields, c->stream), "efield kernel");
+    ++c->launches;
+    c->e_stale = false;
+    c->split_stale = shifted(c);
+    return EK_OK;
 }
 
 int ctx_residual_buffers(ek_ctx *c) {

@@ -44,6 +44,7 @@ struct ek_ctx {
     long long wait_cycles = 1ll << 31;    // EK_OPT_WAIT_CYCLES
     bool keep_l2 = false;                 // rhs + psi planes fit the L2 share kept for them
     int *err_dev = nullptr;               // set by bounded device waits
+    unsigned long long *jacobi_word = nullptr;  // ek_poisson_jacobi: largest change of a sweep
     ek::Rates *rates_dev = nullptr;
     ek::Rates rates{};
     ek::PoissonPlan pp{};
@@ -66,4 +67,7 @@ void ctx_refresh(ek_ctx *c);
 int ctx_residual_buffers(ek_ctx *c);
 int ctx_residual_finish(ek_ctx *c, const double *sums, int32_t interval, double *out5);
 bool ctx_poisson_f32(const ek_ctx *c);  // the FP32 form runs for this context
+// After psi was set on the device outside a step (a grid relaxation): the E
+// planes from psi, and the FP32 planes of shifted storage marked stale.
+int ctx_after_psi(ek_ctx *c);
 }  // namespace ek

@@ -76,6 +76,8 @@ _SIGS = {
     "ek_tile_x": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "ek_step": ([ctypes.c_void_p, ctypes.c_int32], ctypes.c_int),
     "ek_poisson": ([ctypes.c_void_p], ctypes.c_int),
+    "ek_poisson_jacobi": ([ctypes.c_void_p, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
+                           _P(ctypes.c_int32), _dp], ctypes.c_int),
     "ek_get_fields": ([ctypes.c_void_p] + [_dp] * 8, ctypes.c_int),
     "ek_get_fields_device": ([ctypes.c_void_p] + [ctypes.c_void_p] * 8, ctypes.c_int),
     "ek_residual": ([ctypes.c_void_p, ctypes.c_int32, _dp], ctypes.c_int),

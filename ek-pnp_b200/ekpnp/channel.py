@@ -152,6 +152,17 @@ class Channel:
 
     fast_Poisson = poisson
 
+    def poisson_jacobi(self, max_sweeps=1_000_000, tol=1e-9, omega=1.0, check_every=100):
+        """Grid relaxation of the Poisson equation from the current psi (the
+        reference's poisson_phi, made schedule-independent); returns (sweeps,
+        last measured largest change)."""
+        n, ch = ctypes.c_int32(0), ctypes.c_double(0.0)
+        check(lib().ek_poisson_jacobi(self._h, int(max_sweeps), float(tol), float(omega), int(check_every),
+                                      ctypes.byref(n), ctypes.byref(ch)))
+        return int(n.value), float(ch.value)
+
+    poisson_phi = poisson_jacobi
+
     def sync(self):
         check(lib().ek_sync(self._h))
 

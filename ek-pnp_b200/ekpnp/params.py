@@ -97,7 +97,12 @@ def batch_specs(count=512, seed=2, nx_choices=BATCH_NX, ny_range=(32, 512), kapp
     default_rng(seed), per channel in this order: nx from nx_choices, ny
     uniform integer in ny_range (inclusive), kappa*H log-uniform, zeta
     uniform, E_x log-uniform, D uniform."""
-    rng = np.random.default_rng(seed)
+    return _draw_specs(np.random.default_rng(seed), count, nx_choices, ny_range, kappa_h_range, zeta_range,
+                       ex_range, diff_range, eps)
+
+
+def _draw_specs(rng, count, nx_choices=BATCH_NX, ny_range=(32, 512), kappa_h_range=(1.0, 50.0),
+                zeta_range=(-4.0, -0.5), ex_range=(1e-5, 1e-3), diff_range=(0.02, 0.1), eps=BATCH_EPS):
     out = []
     for _ in range(int(count)):
         nx = int(rng.choice(np.asarray(nx_choices)))
@@ -109,6 +114,21 @@ def batch_specs(count=512, seed=2, nx_choices=BATCH_NX, ny_range=(32, 512), kapp
         out.append(dict(nx=nx, ny=ny, kappa_h=kh, zeta=zeta, ex=ex, diff=diff, eps=float(eps),
                         rest_quirk=BATCH_REST_QUIRK))
     return out
+
+
+def batch_noisy_states(count=512, seed=2, rho0=1.0, c0=1.0, **ranges):
+    """Start fields of the batch_specs(count, seed, **ranges) channels: u = psi
+    = 0, rho = rho0, c+- = c0 (1 + 1e-3 N(0, 1)), the normal deviates drawn
+    from the same default_rng(seed) stream right after the channel
+    parameters, per channel an (ny, nx) array for c+ then one for c- (a
+    generator: one channel's fields at a time)."""
+    rng = np.random.default_rng(seed)
+    for s in _draw_specs(rng, count, **ranges):
+        nx, ny = s["nx"], s["ny"]
+        cp = c0 * (1.0 + 1e-3 * rng.standard_normal((ny, nx)))
+        cn = c0 * (1.0 + 1e-3 * rng.standard_normal((ny, nx)))
+        z = np.zeros((ny, nx))
+        yield dict(rho=np.full((ny, nx), rho0), ux=z, uy=z.copy(), cp=cp, cn=cn, psi=z.copy())
 
 
 def spec_params(spec, storage):

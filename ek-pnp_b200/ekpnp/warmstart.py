@@ -168,19 +168,23 @@ def run_to_steady(batch, tol=1e-8, check=1000, max_steps=200_000, judge=None, fr
     channels stop stepping once converged or diverged (and, with judge, once
     judged), so the work shrinks as they finish.  Returns per-channel steps to
     steady (-1: not reached), a diverged mask, the residual history (one row
-    per check; frozen channels repeat their last value) and the wall time in
-    seconds (host clock, checks included).  judge=(k1, k2): also return the
-    channels whose worst residual rose from check k1 to check k2."""
+    per check; frozen channels repeat their last value), the wall time in
+    seconds (host clock, checks included) and the node updates of the stepping
+    channels (node_steps).  judge=(k1, k2): also return the channels whose
+    worst residual rose from check k1 to check k2."""
     n = len(batch)
     steps_to = np.full(n, -1, dtype=np.int64)
     hist = []
     done = np.zeros(n, bool)
     last = np.full(n, np.inf)
+    node_steps = 0
     batch.sync()
     t0 = time.perf_counter()
     batch.residual(check)  # first snapshot
     while batch.steps < max_steps:
-        batch.step(min(check, max_steps - batch.steps))
+        k = min(check, max_steps - batch.steps)
+        node_steps += batch.active[1] * k
+        batch.step(k)
         r = batch.residual(check)[:, 4]
         r = np.where(done, last, r)
         last = r
@@ -201,7 +205,7 @@ def run_to_steady(batch, tol=1e-8, check=1000, max_steps=200_000, judge=None, fr
     hist = np.array(hist)
     diverged = ~np.isfinite(hist[-1]) if len(hist) else np.zeros(n, bool)
     rising = None if judge is None else rising_channels(hist, *judge)
-    return dict(steps=steps_to, diverged=diverged, history=hist, wall_s=wall, rising=rising)
+    return dict(steps=steps_to, diverged=diverged, history=hist, wall_s=wall, rising=rising, node_steps=node_steps)
 
 
 def rising_channels(hist, k1, k2):

@@ -223,6 +223,21 @@ int ek_set_option(ek_ctx *ctx, int32_t option, int64_t value);
  * fast_Poisson (poisson.cu:180-208) without its per-call cudaMalloc/Free. */
 int ek_poisson(ek_ctx *ctx);
 
+/* Grid relaxation of the same Poisson equation for the current c+, c-
+ * moments: poisson_phi / gpu_poisson (poisson.cu:35-130), the reference's
+ * iterative solver, which its time loop does not call.  Weighted Jacobi
+ * sweeps (omega in (0, 2), 1 = the reference's update) from the current
+ * psi, walls at the wall potentials, until the largest change of a sweep is
+ * below tol (the reference: 1e-9) or max_sweeps (the reference: 1e6); the
+ * change is measured every check_every sweeps and on the last.  Unlike the
+ * reference's in-place update, every sweep reads one buffer and writes
+ * another, so the result does not depend on the schedule.  The fixed point
+ * is the five-point discretisation (three-point along x too), not the
+ * spectral-x one of ek_poisson.  Then E from psi.  sweeps / change (optional): sweeps done and the last measured change
+ * (-1 if none was measured).  Returns EK_OK whether or not tol was reached. */
+int ek_poisson_jacobi(ek_ctx *ctx, int32_t max_sweeps, double tol, double omega, int32_t check_every,
+                      int32_t *sweeps, double *change);
+
 /* Copy the macroscopic fields of the last step to host arrays (any pointer may
  * be NULL).  rho, ux, uy, cp, cn are the moments of the last step's
  * pre-collision populations, psi/ex/ey the Poisson result from them, as the

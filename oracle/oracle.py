@@ -129,3 +129,59 @@ class OracleChannel:
         f, h, t = (np.empty(9 * n) for _ in range(3))
         lib().ekor_get_populations(self._h, _ptr(f), _ptr(h), _ptr(t))
         return [a.reshape(9, self.ny, self.nx) for a in (f, h, t)]
+
+
+def jacobi_poisson(params, cp, cn, psi0, zlo, zhi, sweeps, omega=1.0):
+    """Grid relaxation of the channel's Poisson equation, numpy FP64:
+    gpu_poisson's five-point update (poisson.cu:75-130) written for dx != dy
+    and made deterministic (each sweep reads the previous iterate only):
+        psi = ((L + R)/dx^2 + (U + D)/dy^2 - rhs) / (2/dx^2 + 2/dy^2),
+        rhs = -f_charge (c+ - c-) / eps,
+    relaxed by omega, periodic in x, rows 0 and ny-1 held at zlo(x), zhi(x)
+    (voltage / voltage2 in the reference, poisson.cu:99-106).  Returns the
+    iterate after `sweeps` sweeps and the largest change of the last one."""
+    p = params
+    idx2, idy2 = 1.0 / (p["dx"] * p["dx"]), 1.0 / (p["dy"] * p["dy"])
+    rhs = -p["f_charge"] * (np.asarray(cp) - np.asarray(cn)) / p["eps"]
+    a = np.array(psi0, dtype=np.float64, copy=True)
+    a[0], a[-1] = zlo, zhi
+    change = 0.0
+    for _ in range(int(sweeps)):
+        c = a[1:-1]
+        fit = ((np.roll(c, 1, axis=1) + np.roll(c, -1, axis=1)) * idx2 + (a[:-2] + a[2:]) * idy2
+               - rhs[1:-1]) / (2.0 * idx2 + 2.0 * idy2)
+        new = c + omega * (fit - c)
+        change = float(np.abs(new - c).max())
+        a = a.copy()
+        a[1:-1] = new
+    return a, change
+
+
+def five_point_poisson(params, cp, cn, zlo, zhi):
+    """Direct solve of the five-point system whose fixed point jacobi_poisson
+    relaxes to: per x-mode m the three-point x-symbol (4/dx^2) sin^2(pi m/nx)
+    (where the spectral solve has kx^2), then the tridiagonal y-system with the
+    walls lifted into the first and last interior rows.  numpy FP64."""
+    from scipy.linalg import solve_banded
+    p = params
+    ny, nx = np.asarray(cp).shape
+    idy2 = 1.0 / (p["dy"] * p["dy"])
+    rhs = -p["f_charge"] * (np.asarray(cp) - np.asarray(cn))[1:-1] / p["eps"]
+    rhs = rhs.astype(np.complex128)
+    zlo, zhi = np.broadcast_to(zlo, (nx,)), np.broadcast_to(zhi, (nx,))
+    rhs[0] -= zlo * idy2
+    rhs[-1] -= zhi * idy2
+    s = np.fft.fft(rhs, axis=1)
+    lam = 4.0 / (p["dx"] * p["dx"]) * np.sin(np.pi * np.arange(nx) / nx) ** 2
+    n = ny - 2
+    out = np.empty_like(s)
+    for m in range(nx):
+        ab = np.zeros((3, n))
+        ab[0, 1:] = idy2
+        ab[1] = -2.0 * idy2 - lam[m]
+        ab[2, :-1] = idy2
+        out[:, m] = solve_banded((1, 1), ab, s[:, m])
+    psi = np.empty((ny, nx))
+    psi[1:-1] = np.fft.ifft(out, axis=1).real
+    psi[0], psi[-1] = zlo, zhi
+    return psi
