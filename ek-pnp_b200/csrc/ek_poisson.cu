@@ -735,84 +735,78 @@ __global__ void __launch_bounds__(TB_THREADS) tridiag_part(const PoissonPlan pp,
 }
 
 // Shared memory of the FP32 form's column kernel: the FP32 modes' segment
-// ends, or the FP64 zero mode's (real) affine maps.
+// ends, or the zero mode's per-warp scan totals.
 union ColumnShared {
     TridiagSharedT<float, float2> f;
-    struct {
-        double e[TB_THREADS];
-        double f[TB_THREADS];
-    } z;
+    double wtot[TB_THREADS / 32];
 };
 
-// Value entering this thread's segment of the zero mode: the real affine maps
-// D -> e + f D of the block's TB_THREADS segments composed in order (forward
-// from segment 0 or backward from the last), log2(TB_THREADS) rounds.
-template <bool FWD>
-__device__ __forceinline__ double zero_carry(double e, double f, ColumnShared &sh) {
-    const int t = threadIdx.x;
-    for (int off = 1; off < TB_THREADS; off <<= 1) {
-        sh.z.e[t] = e;
-        sh.z.f[t] = f;
-        __syncthreads();
-        const int src = FWD ? t - off : t + off;
-        if (FWD ? src >= 0 : src < TB_THREADS) {
-            e = e + f * sh.z.e[src];
-            f = f * sh.z.f[src];
-        }
-        __syncthreads();
+// Inclusive sum of v over threads 0..threadIdx.x of the block (TB_THREADS
+// threads): warp shuffles, then the warp totals in shared memory.  Every
+// thread of the block calls it; *total gets the block's sum.
+__device__ __forceinline__ double block_scan(double v, ColumnShared &sh, double *total) {
+    constexpr int NW = TB_THREADS / 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const double t = __shfl_up_sync(0xffffffffu, v, off);
+        if (lane >= off) v += t;
     }
-    sh.z.e[t] = e;
+    if (lane == 31) sh.wtot[w] = v;
     __syncthreads();
-    const int prev = FWD ? t - 1 : t + 1;
-    const double out = (FWD ? prev >= 0 : prev < TB_THREADS) ? sh.z.e[prev] : 0.0;
+    if (w == 0) {
+        double t = lane < NW ? sh.wtot[lane] : 0.0;
+#pragma unroll
+        for (int off = 1; off < NW; off <<= 1) {
+            const double u = __shfl_up_sync(0xffffffffu, t, off);
+            if (lane >= off) t += u;
+        }
+        if (lane < NW) sh.wtot[lane] = t;
+    }
     __syncthreads();
-    return out;
+    if (w > 0) v += sh.wtot[w - 1];
+    *total = sh.wtot[NW - 1];
+    __syncthreads();  // sh is written again by the next call
+    return v;
 }
 
 // The zero mode (kx = 0) of the FP32 form's column solve in FP64, by one
-// block: thread t owns rows [t L, t L + L) of column 0 of the FP64 spectrum
-// (the row sums, real), L = ceil(n / TB_THREADS).  The partitioned Thomas
-// solve of tridiag_part_gen with the channel's FP64 pivots, but working on
-// the column in place (L2-resident, 8 n bytes) rather than in registers, so
-// that it fits the FP32 kernel's register budget.
+// block.  Its system phi_{j-1} - 2 phi_j + phi_{j+1} = h_j, h_j = dy^2 S_j
+// (S_j: the row sums in column 0 of the FP64 spectrum), phi_{-1} = phi_n = 0,
+// is solved exactly by two prefix sums: with H_k = h_0 + ... + h_k,
+//     phi_j = (j + 1) g_0 + (H_0 + ... + H_{j-1}),  g_0 = -(H_0 + ... + H_{n-1}) / (n + 1)
+// (g_j = phi_j - phi_{j-1} steps by h_j).  Thread t owns rows [t L, t L + L),
+// L = ceil(n / TB_THREADS), and reads them three times (the later reads hit
+// L1), so the block holds no per-row registers and fits the FP32 kernel's
+// budget; the two sums over the threads are block scans.
 __device__ __forceinline__ void zero_mode_f64(const PoissonPlan &pp, ColumnShared &sh) {
     const int n = pp.n, L = (n + TB_THREADS - 1) / TB_THREADS;
     const int ja = (int)threadIdx.x * L, cnt = max(0, min(n, ja + L) - ja);
-    const size_t mp = (size_t)pp.mp;
-    double *col = &pp.spec[0].x;  // element j at col[2 j mp]
-    const double *piv = pp.piv;
+    const size_t stride = 2 * (size_t)pp.mp;  // element j of the column at col[j * stride]
+    double *col = &pp.spec[0].x;
     const double dy2 = pp.dy2;
-    // forward sweep of the segment from a zero entry value
-    double d = 0.0, mu = 1.0;
+    // segment sum of h, then H at the segment's start
+    double s1 = 0.0;
+    for (int q = 0; q < cnt; ++q) s1 += dy2 * __ldg(col + (size_t)(ja + q) * stride);
+    double tot;
+    const double h0 = block_scan(s1, sh, &tot) - s1;  // H_{ja - 1}
+    // segment sum of H, then the sum of H before the segment and over all rows
+    double H = h0, s2 = 0.0;
     for (int q = 0; q < cnt; ++q) {
-        const size_t j = (size_t)(ja + q) * mp;
-        const double c = piv[j];
-        d = (dy2 * col[2 * j] - d) * c;
-        mu = -c * mu;
-        col[2 * j] = d;
+        H += dy2 * __ldg(col + (size_t)(ja + q) * stride);
+        s2 += H;
     }
-    const double D = zero_carry<true>(d, mu, sh);
-    // true forward values, then the backward sweep from a zero exit value
-    mu = 1.0;
+    double S;
+    const double G0 = block_scan(s2, sh, &S) - s2;  // H_0 + ... + H_{ja - 1}
+    const double g0 = -S / (double)(n + 1);
+    H = h0;
+    double G = G0;
     for (int q = 0; q < cnt; ++q) {
-        const size_t j = (size_t)(ja + q) * mp;
-        mu = -piv[j] * mu;
-        col[2 * j] += mu * D;
-    }
-    double x = 0.0, nu = 1.0;
-    for (int q = cnt - 1; q >= 0; --q) {
-        const size_t j = (size_t)(ja + q) * mp;
-        const double c = piv[j];
-        x = col[2 * j] - c * x;
-        nu = -c * nu;
-        col[2 * j] = x;
-    }
-    const double X = zero_carry<false>(x, nu, sh);
-    nu = 1.0;
-    for (int q = cnt - 1; q >= 0; --q) {
-        const size_t j = (size_t)(ja + q) * mp;
-        nu = -piv[j] * nu;
-        col[2 * j] += nu * X;
+        const int j = ja + q;
+        const double hj = dy2 * __ldg(col + (size_t)j * stride);
+        col[(size_t)j * stride] = (double)(j + 1) * g0 + G;
+        H += hj;
+        G += H;
     }
 }
 
