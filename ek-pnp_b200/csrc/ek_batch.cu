@@ -80,7 +80,8 @@ batch_lbm(const ChanF *__restrict__ chans, const S *const *__restrict__ src, S *
             const int r = threadIdx.x / tl.w;
             const int x = tl.z + (threadIdx.x - r * tl.w), y = tl.y + r;
             if (r < TXB / tl.w && x < ks.nx && y < ks.ny)
-                node_shifted<S, FIRST, EE>(ks, src[cur], dst[cur], fields[cur], x, y, mom, sbuf);
+                // 32-bit indexing: batched channels are at most 4096 x 8194 (ek_batch_create)
+                node_shifted<S, FIRST, EE, uint32_t>(ks, src[cur], dst[cur], fields[cur], x, y, mom, sbuf);
         }
         __syncthreads();  // every thread has read `claim` before thread 0 claims again
     }
@@ -510,6 +511,7 @@ int ek_batch_create(const ek_params *params, int32_t count, ek_batch **out) {
             return ek::ctx_fail(EK_ERR_INVALID, "all channels of a batch need one storage mode");
         if (p.storage != EK_STORE_F32 && p.storage != EK_STORE_F16)
             return ek::ctx_fail(EK_ERR_UNSUPPORTED, "batches use FP32 or FP16 storage");
+        static_assert(index32_fits((size_t)4096 * 8194), "batched channels use 32-bit indexing");
         if (!pow2(p.nx) || p.nx < 16 || p.nx > 4096)
             return ek::ctx_fail(EK_ERR_UNSUPPORTED, "batched channels need nx a power of two in [16, 4096]");
         if (p.flags & EK_FLAG_EXPLICIT_E) return ek::ctx_fail(EK_ERR_UNSUPPORTED, "batches derive E from psi");

@@ -80,13 +80,15 @@ constexpr int TPB = 128;
 #define EK_LBM_MIN_BLOCKS 7
 #endif
 
-template <typename S, bool FIRST, bool EE>
+// I: the index type of the node update (uint32_t when every offset into the
+// population and field planes fits 32 bits, see own9s).
+template <typename S, bool FIRST, bool EE, typename I>
 __global__ void __launch_bounds__(TPB, EK_LBM_MIN_BLOCKS)
 step_shifted(const ChanF k, const S *__restrict__ src, S *__restrict__ dst, double *__restrict__ fields, bool mom,
              int sbuf) {
     const int x = blockIdx.x * TPB + threadIdx.x;
     if (x >= k.nx) return;
-    node_shifted<S, FIRST, EE>(k, src, dst, fields, x, blockIdx.y, mom, sbuf);
+    node_shifted<S, FIRST, EE, I>(k, src, dst, fields, x, blockIdx.y, mom, sbuf);
 }
 
 template <typename S>
@@ -109,20 +111,27 @@ __global__ void __launch_bounds__(256) wall_delta(const ChanF k, const float *__
     if (i < 4 * k.nx) wall_delta_dev(k, kwall, wdelta, i);
 }
 
-template <typename S>
-cudaError_t step_typed(const ChanF &k, const void *src, void *dst, double *fields, bool first, bool ee,
-                       bool mom, int sbuf, cudaStream_t s) {
+template <typename S, typename I>
+cudaError_t step_indexed(const ChanF &k, const void *src, void *dst, double *fields, bool first, bool ee,
+                         bool mom, int sbuf, cudaStream_t s) {
     const dim3 g((k.nx + TPB - 1) / TPB, k.ny);
     const S *a = (const S *)src;
     S *b = (S *)dst;
     if (first) {
-        if (ee) step_shifted<S, true, true><<<g, TPB, 0, s>>>(k, a, b, fields, mom, sbuf);
-        else step_shifted<S, true, false><<<g, TPB, 0, s>>>(k, a, b, fields, mom, sbuf);
+        if (ee) step_shifted<S, true, true, I><<<g, TPB, 0, s>>>(k, a, b, fields, mom, sbuf);
+        else step_shifted<S, true, false, I><<<g, TPB, 0, s>>>(k, a, b, fields, mom, sbuf);
     } else {
-        if (ee) step_shifted<S, false, true><<<g, TPB, 0, s>>>(k, a, b, fields, mom, sbuf);
-        else step_shifted<S, false, false><<<g, TPB, 0, s>>>(k, a, b, fields, mom, sbuf);
+        if (ee) step_shifted<S, false, true, I><<<g, TPB, 0, s>>>(k, a, b, fields, mom, sbuf);
+        else step_shifted<S, false, false, I><<<g, TPB, 0, s>>>(k, a, b, fields, mom, sbuf);
     }
     return cudaGetLastError();
+}
+
+template <typename S>
+cudaError_t step_typed(const ChanF &k, const void *src, void *dst, double *fields, bool first, bool ee,
+                       bool mom, int sbuf, cudaStream_t s) {
+    if (index32_fits(k.plane)) return step_indexed<S, uint32_t>(k, src, dst, fields, first, ee, mom, sbuf, s);
+    return step_indexed<S, size_t>(k, src, dst, fields, first, ee, mom, sbuf, s);
 }
 
 __global__ void __launch_bounds__(256) row_refs(const Chan c, const double *__restrict__ fields, int qf, int qp,

@@ -101,25 +101,32 @@ template <> __device__ __forceinline__ void st_pop<__half>(__half *p, float v) {
 
 constexpr float W0F = 4.0f / 9.0f, WSF = 1.0f / 9.0f, WDF = 1.0f / 36.0f;
 
-template <typename S>
-__device__ __forceinline__ void own9s(const S *__restrict__ b, size_t pl, size_t o, float p[9]) {
+// Index arithmetic of the node update in type I: size_t in general,
+// uint32_t where every offset into the 27 population planes and the 9 field
+// planes fits 32 bits (27 plane < 2^32), which spares the 64-bit address
+// arithmetic of every access.
+// Whether the 32-bit index form covers a channel of `plane` elements a plane.
+__host__ __device__ constexpr bool index32_fits(size_t plane) { return plane < ((size_t)1 << 32) / 27; }
+
+template <typename S, typename I = size_t>
+__device__ __forceinline__ void own9s(const S *__restrict__ b, I pl, I o, float p[9]) {
 #pragma unroll
-    for (int d = 0; d < 9; ++d) p[d] = ld_pop<S>(b + d * pl + o);
+    for (int d = 0; d < 9; ++d) p[d] = ld_pop<S>(b + ((I)d * pl + o));
 }
 
-template <typename S>
-__device__ __forceinline__ void pull9s(const S *__restrict__ b, size_t pl, int nxp, int x, int y, int xm,
+template <typename S, typename I = size_t>
+__device__ __forceinline__ void pull9s(const S *__restrict__ b, I pl, int nxp, int x, int y, int xm,
                                        int xp, int ym, int yp, float p[9]) {
-    const size_t r0 = (size_t)y * nxp, rm = (size_t)ym * nxp, rp = (size_t)yp * nxp;
-    p[0] = ld_pop<S>(b + r0 + x);
-    p[1] = ld_pop<S>(b + 1 * pl + r0 + xm);
-    p[2] = ld_pop<S>(b + 2 * pl + rm + x);
-    p[3] = ld_pop<S>(b + 3 * pl + r0 + xp);
-    p[4] = ld_pop<S>(b + 4 * pl + rp + x);
-    p[5] = ld_pop<S>(b + 5 * pl + rm + xm);
-    p[6] = ld_pop<S>(b + 6 * pl + rm + xp);
-    p[7] = ld_pop<S>(b + 7 * pl + rp + xp);
-    p[8] = ld_pop<S>(b + 8 * pl + rp + xm);
+    const I r0 = (I)y * (I)nxp, rm = (I)ym * (I)nxp, rp = (I)yp * (I)nxp;
+    p[0] = ld_pop<S>(b + (r0 + (I)x));
+    p[1] = ld_pop<S>(b + (1 * pl + r0 + (I)xm));
+    p[2] = ld_pop<S>(b + (2 * pl + rm + (I)x));
+    p[3] = ld_pop<S>(b + (3 * pl + r0 + (I)xp));
+    p[4] = ld_pop<S>(b + (4 * pl + rp + (I)x));
+    p[5] = ld_pop<S>(b + (5 * pl + rm + (I)xm));
+    p[6] = ld_pop<S>(b + (6 * pl + rm + (I)xp));
+    p[7] = ld_pop<S>(b + (7 * pl + rp + (I)xp));
+    p[8] = ld_pop<S>(b + (8 * pl + rp + (I)xm));
 }
 
 // Change of frame of pulled populations to the puller's row reference:
@@ -300,12 +307,13 @@ __device__ __forceinline__ void efield_shifted(const ChanF &k, const double *__r
 // FP32 fluctuations alone, Ey from the FP64 difference of the two row means
 // (the zero mode, rounded once) plus that of the fluctuations.  Stencil of
 // gpu_efield / gpu_bc (poisson.cu:145-174).
+template <typename I = size_t>
 __device__ __forceinline__ void efield_f32(const ChanF &k, int x, int y, int xm, int xp, float *ex, float *ey) {
-    const size_t r = (size_t)y * k.nxp;
-    *ex = (__ldg(k.psif + r + xm) - __ldg(k.psif + r + xp)) * k.half_inv_dxf;
+    const I r = (I)y * (I)k.nxp;
+    *ex = (__ldg(k.psif + (r + (I)xm)) - __ldg(k.psif + (r + (I)xp))) * k.half_inv_dxf;
     const int yc = y == 0 ? 1 : (y == k.ny - 1 ? k.ny - 2 : y);
     const float eym = (float)((__ldg(k.psim + yc - 1) - __ldg(k.psim + yc + 1)) * k.half_inv_dy);
-    *ey = eym + (__ldg(k.psif + (size_t)(yc - 1) * k.nxp + x) - __ldg(k.psif + (size_t)(yc + 1) * k.nxp + x)) *
+    *ey = eym + (__ldg(k.psif + ((I)(yc - 1) * (I)k.nxp + (I)x)) - __ldg(k.psif + ((I)(yc + 1) * (I)k.nxp + (I)x))) *
                     k.half_inv_dyf;
 }
 
@@ -314,28 +322,28 @@ __device__ __forceinline__ void efield_f32(const ChanF &k, int x, int y, int xm,
 // Raw populations of one node, as stored: FIRST -> the node's own
 // (pre-collision) values; otherwise the fluid pulled from the neighbours and
 // the ions pulled (interior rows) or the node's own values (wall rows).
-template <typename S, bool FIRST>
+template <typename S, bool FIRST, typename I = size_t>
 __device__ __forceinline__ void gather_global(const ChanF &k, const S *__restrict__ src, int x, int y, float f[9],
                                               float h[9], float t[9]) {
-    const size_t pl = k.plane;
+    const I pl = (I)k.plane;
     const int nxp = k.nxp;
-    const size_t o = (size_t)y * nxp + x;
+    const I o = (I)y * (I)nxp + (I)x;
     const bool wall = y == 0 || y == k.ny - 1;
     const int xm = x == 0 ? k.nx - 1 : x - 1, xp = x + 1 == k.nx ? 0 : x + 1;
     const int ym = y == 0 ? k.ny - 1 : y - 1, yp = y + 1 == k.ny ? 0 : y + 1;
     const S *sf = src, *sh = src + 9 * pl, *st = src + 18 * pl;
     if (FIRST) {
-        own9s<S>(sf, pl, o, f);
-        own9s<S>(sh, pl, o, h);
-        own9s<S>(st, pl, o, t);
+        own9s<S, I>(sf, pl, o, f);
+        own9s<S, I>(sh, pl, o, h);
+        own9s<S, I>(st, pl, o, t);
     } else {
-        pull9s<S>(sf, pl, nxp, x, y, xm, xp, ym, yp, f);
+        pull9s<S, I>(sf, pl, nxp, x, y, xm, xp, ym, yp, f);
         if (wall) {
-            own9s<S>(sh, pl, o, h);
-            own9s<S>(st, pl, o, t);
+            own9s<S, I>(sh, pl, o, h);
+            own9s<S, I>(st, pl, o, t);
         } else {
-            pull9s<S>(sh, pl, nxp, x, y, xm, xp, ym, yp, h);
-            pull9s<S>(st, pl, nxp, x, y, xm, xp, ym, yp, t);
+            pull9s<S, I>(sh, pl, nxp, x, y, xm, xp, ym, yp, h);
+            pull9s<S, I>(st, pl, nxp, x, y, xm, xp, ym, yp, t);
         }
     }
 }
@@ -349,13 +357,13 @@ __device__ __forceinline__ void gather_global(const ChanF &k, const S *__restric
 // so a step that wrote the moments could round differently from one that
 // did not.  One body with predicated stores keeps every step's arithmetic
 // independent of how the steps are split into calls.
-template <typename S, bool FIRST, bool EXPLICIT_E>
+template <typename S, bool FIRST, bool EXPLICIT_E, typename I = size_t>
 __device__ __forceinline__ void collide_shifted(const ChanF &k, float f[9], float h[9], float t[9],
                                                 const S *__restrict__ src, S *__restrict__ dst,
                                                 double *__restrict__ fields, int x, int y, bool moments, int sbuf) {
-    const size_t pl = k.plane;
+    const I pl = (I)k.plane;
     const int nxp = k.nxp;
-    const size_t o = (size_t)y * nxp + x;
+    const I o = (I)y * (I)nxp + (I)x;
     const bool lo = y == 0, hi = y == k.ny - 1, wall = lo || hi;
     const int xm = x == 0 ? k.nx - 1 : x - 1, xp = x + 1 == k.nx ? 0 : x + 1;
     const int ym = y == 0 ? k.ny - 1 : y - 1, yp = y + 1 == k.ny ? 0 : y + 1;
@@ -410,7 +418,7 @@ __device__ __forceinline__ void collide_shifted(const ChanF &k, float f[9], floa
         ex = (float)fields[F_EX * pl + o];
         ey = (float)fields[F_EY * pl + o];
     } else {
-        efield_f32(k, x, y, xm, xp, &ex, &ey);
+        efield_f32<I>(k, x, y, xm, xp, &ex, &ey);
     }
     float fx = 0.0f, fy = 0.0f;
     const float dq = dcp - dcn;
@@ -425,12 +433,12 @@ __device__ __forceinline__ void collide_shifted(const ChanF &k, float f[9], floa
     float uy = (momy(f) * k.inv_cfl + fy * k.half_dt) * rrho;
     if (lo) {
         float m[9];
-        const size_t o1 = (size_t)nxp + x;
+        const I o1 = (I)nxp + (I)x;
         const float kf1 = __ldg(k.kref + 1);
         if (FIRST) {
-            own9s<S>(sf, pl, o1, m);
+            own9s<S, I>(sf, pl, o1, m);
         } else {
-            pull9s<S>(sf, pl, nxp, x, 1, xm, xp, 0, 2, m);
+            pull9s<S, I>(sf, pl, nxp, x, 1, xm, xp, 0, 2, m);
             reframe(m, __ldg(k.kref + 0) - kf1, __ldg(k.kref + 2) - kf1);
         }
         const float rrho1 = 1.0f / (36.0f * kf1 + sum9f(m));
@@ -438,11 +446,11 @@ __device__ __forceinline__ void collide_shifted(const ChanF &k, float f[9], floa
         uy = -(momy(m) * k.inv_cfl + fy * k.half_dt) * rrho1;
     }
     if (moments) {
-        fields[F_RHO * pl + o] = (double)Rf + (double)drho;
-        fields[F_UX * pl + o] = ux;
-        fields[F_UY * pl + o] = uy;
-        fields[F_CP * pl + o] = (double)Rh + (double)dcp;
-        fields[F_CN * pl + o] = (double)Rt + (double)dcn;
+        fields[(I)F_RHO * pl + o] = (double)Rf + (double)drho;
+        fields[(I)F_UX * pl + o] = ux;
+        fields[(I)F_UY * pl + o] = uy;
+        fields[(I)F_CP * pl + o] = (double)Rh + (double)dcp;
+        fields[(I)F_CN * pl + o] = (double)Rt + (double)dcn;
     }
     // right-hand side without its FP64 row constant (rhs_q (R+ - R-) and the
     // lifting's x-mean, added by the row pass), with the lifting's x-fluctuation
@@ -457,37 +465,35 @@ __device__ __forceinline__ void collide_shifted(const ChanF &k, float f[9], floa
         {
             const float vx = ux + k.mob_p * ex, vy = uy + k.mob_p * ey;
             trt_f32<false, false>(h, dcp, Rh + dcp, vx, vy, vx * vx + vy * vy, k.wcp, k.wcm, k, 0.0f, 0.0f, 0.0f, 0.0f);
-            S *dh = dst + 9 * pl;
 #pragma unroll
-            for (int d = 0; d < 9; ++d) st_pop<S>(dh + d * pl + o, h[d]);
+            for (int d = 0; d < 9; ++d) st_pop<S>(dst + ((I)(9 + d) * pl + o), h[d]);
         }
         {
             const float vx = ux + k.mob_n * ex, vy = uy + k.mob_n * ey;
             trt_f32<false, false>(t, dcn, Rt + dcn, vx, vy,
                                   (k.flags & EK_FLAG_REST_QUIRK) ? ux * ux + uy * uy : vx * vx + vy * vy, k.wtp, k.wtm,
                                   k, 0.0f, 0.0f, 0.0f, 0.0f);
-            S *dt_ = dst + 18 * pl;
 #pragma unroll
-            for (int d = 0; d < 9; ++d) st_pop<S>(dt_ + d * pl + o, t[d]);
+            for (int d = 0; d < 9; ++d) st_pop<S>(dst + ((I)(18 + d) * pl + o), t[d]);
         }
     }
     S *df = dst;
     if (lo) {
         st_pop<S>(df + o, f[0]);
 #pragma unroll
-        for (int d = 1; d < 9; ++d) st_pop<S>(df + oppd(d) * pl + o, f[d]);
+        for (int d = 1; d < 9; ++d) st_pop<S>(df + ((I)oppd(d) * pl + o), f[d]);
         return;
     }
     if (hi) {
         st_pop<S>(df + o, f[0]);
-        st_pop<S>(df + 3 * pl + o, f[1] - k.ms);
-        st_pop<S>(df + 4 * pl + o, f[2]);
-        st_pop<S>(df + 1 * pl + o, f[3] + k.ms);
-        st_pop<S>(df + 2 * pl + o, f[4]);
-        st_pop<S>(df + 7 * pl + o, f[5] - k.md);
-        st_pop<S>(df + 8 * pl + o, f[6] + k.md);
-        st_pop<S>(df + 5 * pl + o, f[7] + k.md);
-        st_pop<S>(df + 6 * pl + o, f[8] - k.md);
+        st_pop<S>(df + (3 * pl + o), f[1] - k.ms);
+        st_pop<S>(df + (4 * pl + o), f[2]);
+        st_pop<S>(df + (1 * pl + o), f[3] + k.ms);
+        st_pop<S>(df + (2 * pl + o), f[4]);
+        st_pop<S>(df + (7 * pl + o), f[5] - k.md);
+        st_pop<S>(df + (8 * pl + o), f[6] + k.md);
+        st_pop<S>(df + (5 * pl + o), f[7] + k.md);
+        st_pop<S>(df + (6 * pl + o), f[8] - k.md);
         return;
     }
     // fluid: FP32 TRT with the Guo source, moment form (trt_f32); the
@@ -498,15 +504,15 @@ __device__ __forceinline__ void collide_shifted(const ChanF &k, float f[9], floa
     else
         trt_f32<false, true>(f, drho, rho, ux, uy, ux * ux + uy * uy, k.wp, k.wm, k, 0.0f, 0.0f, px, py);
 #pragma unroll
-    for (int d = 0; d < 9; ++d) st_pop<S>(df + d * pl + o, f[d]);
+    for (int d = 0; d < 9; ++d) st_pop<S>(df + ((I)d * pl + o), f[d]);
 }
 
-template <typename S, bool FIRST, bool EXPLICIT_E>
+template <typename S, bool FIRST, bool EXPLICIT_E, typename I = size_t>
 __device__ __forceinline__ void node_shifted(const ChanF &k, const S *__restrict__ src, S *__restrict__ dst,
                                              double *__restrict__ fields, int x, int y, bool moments, int sbuf) {
     float f[9], h[9], t[9];
-    gather_global<S, FIRST>(k, src, x, y, f, h, t);
-    collide_shifted<S, FIRST, EXPLICIT_E>(k, f, h, t, src, dst, fields, x, y, moments, sbuf);
+    gather_global<S, FIRST, I>(k, src, x, y, f, h, t);
+    collide_shifted<S, FIRST, EXPLICIT_E, I>(k, f, h, t, src, dst, fields, x, y, moments, sbuf);
 }
 
 // Equilibrium deviations from the fields (pre-collision layout), written to
