@@ -37,26 +37,30 @@ __device__ __forceinline__ double sum9(const double t[9]) {
     return t[0] + t[1] + t[2] + t[3] + t[4] + t[5] + t[6] + t[7] + t[8];
 }
 
-// Load the nine populations stored at (x, y) of one species.
-__device__ __forceinline__ void own9(const double *__restrict__ b, size_t pl, size_t o, double p[9]) {
+// Load the nine populations stored at (x, y) of one species.  I: the index
+// type, uint32_t where the 27 population planes fit 2^32 elements (32-bit
+// offsets from the buffer's base pointer spare the 64-bit address arithmetic).
+template <typename I>
+__device__ __forceinline__ void own9(const double *__restrict__ b, I pl, I o, double p[9]) {
 #pragma unroll
-    for (int d = 0; d < 9; ++d) p[d] = __ldg(b + d * pl + o);
+    for (int d = 0; d < 9; ++d) p[d] = __ldg(b + ((I)d * pl + o));
 }
 
 // Pull: direction d arrives from (x - cx_d, y - cy_d).  xm/xp and ym/yp are
 // the periodic neighbours (gpu_stream wraps x and y, LBM.cu:869-872).
-__device__ __forceinline__ void pull9(const double *__restrict__ b, size_t pl, int nxp, int x,
+template <typename I>
+__device__ __forceinline__ void pull9(const double *__restrict__ b, I pl, int nxp, int x,
                                       int y, int xm, int xp, int ym, int yp, double p[9]) {
-    const size_t r0 = (size_t)y * nxp, rm = (size_t)ym * nxp, rp = (size_t)yp * nxp;
-    p[0] = __ldg(b + r0 + x);
-    p[1] = __ldg(b + 1 * pl + r0 + xm);
-    p[2] = __ldg(b + 2 * pl + rm + x);
-    p[3] = __ldg(b + 3 * pl + r0 + xp);
-    p[4] = __ldg(b + 4 * pl + rp + x);
-    p[5] = __ldg(b + 5 * pl + rm + xm);
-    p[6] = __ldg(b + 6 * pl + rm + xp);
-    p[7] = __ldg(b + 7 * pl + rp + xp);
-    p[8] = __ldg(b + 8 * pl + rp + xm);
+    const I r0 = (I)y * (I)nxp, rm = (I)ym * (I)nxp, rp = (I)yp * (I)nxp;
+    p[0] = __ldg(b + (r0 + (I)x));
+    p[1] = __ldg(b + (1 * pl + r0 + (I)xm));
+    p[2] = __ldg(b + (2 * pl + rm + (I)x));
+    p[3] = __ldg(b + (3 * pl + r0 + (I)xp));
+    p[4] = __ldg(b + (4 * pl + rp + (I)x));
+    p[5] = __ldg(b + (5 * pl + rm + (I)xm));
+    p[6] = __ldg(b + (6 * pl + rm + (I)xp));
+    p[7] = __ldg(b + (7 * pl + rp + (I)xp));
+    p[8] = __ldg(b + (8 * pl + rp + (I)xm));
 }
 
 // Dirichlet anti-bounce-back of one ion species at a wall node, applied to the
@@ -138,16 +142,16 @@ __device__ __forceinline__ void efield_at(const double *__restrict__ psi, const 
     *ey = 0.5 * (__ldg(psi + (size_t)(yc - 1) * c.nxp + x) - __ldg(psi + (size_t)(yc + 1) * c.nxp + x)) / c.dy;
 }
 
-template <bool FIRST, bool EXPLICIT_E, bool MOMENTS>
+template <bool FIRST, bool EXPLICIT_E, bool MOMENTS, typename I>
 __global__ void __launch_bounds__(TPB)
 step_f64(const Chan c, const double *__restrict__ src, double *__restrict__ dst,
          double *__restrict__ fields) {
     const int x = blockIdx.x * TPB + threadIdx.x;
     const int y = blockIdx.y;
     if (x >= c.nx) return;
-    const size_t pl = c.plane;
+    const I pl = (I)c.plane;
     const int nxp = c.nxp;
-    const size_t o = (size_t)y * nxp + x;
+    const I o = (I)y * (I)nxp + (I)x;
     const bool lo = y == 0, hi = y == c.ny - 1;
     const int xm = x == 0 ? c.nx - 1 : x - 1, xp = x + 1 == c.nx ? 0 : x + 1;
     const int ym = y == 0 ? c.ny - 1 : y - 1, yp = y + 1 == c.ny ? 0 : y + 1;
@@ -194,7 +198,7 @@ step_f64(const Chan c, const double *__restrict__ src, double *__restrict__ dst,
     if (lo) {
         // lower wall: minus the velocity of row 1 (LBM.cu:402-443)
         double fm[9];
-        const size_t o1 = (size_t)nxp + x;
+        const I o1 = (I)nxp + (I)x;
         if (FIRST) own9(sf, pl, o1, fm);
         else pull9(sf, pl, nxp, x, 1, xm, xp, 0, 2, fm);
         const double rhoinvm = 1.0 / sum9(fm);
@@ -378,7 +382,13 @@ cudaError_t launch_init_f64(const Chan &c, double *pops, const double *fields, b
 cudaError_t launch_step_f64(const Chan &c, const double *src, double *dst, double *fields,
                             bool first, bool explicit_e, bool moments, cudaStream_t s) {
     const dim3 g = node_grid(c, c.ny);
-#define EK_STEP(F, E, M) step_f64<F, E, M><<<g, TPB, 0, s>>>(c, src, dst, fields)
+    // 32-bit offsets while the 27 population planes fit 2^32 elements
+    const bool i32 = (size_t)27 * c.plane < ((size_t)1 << 32);
+#define EK_STEP(F, E, M)                                                                       \
+    do {                                                                                       \
+        if (i32) step_f64<F, E, M, uint32_t><<<g, TPB, 0, s>>>(c, src, dst, fields);           \
+        else step_f64<F, E, M, size_t><<<g, TPB, 0, s>>>(c, src, dst, fields);                 \
+    } while (0)
     const int key = (first ? 4 : 0) | (explicit_e ? 2 : 0) | (moments ? 1 : 0);
     switch (key) {
         case 0: EK_STEP(false, false, false); break;

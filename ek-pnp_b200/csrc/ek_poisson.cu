@@ -425,7 +425,9 @@ __device__ __forceinline__ void fwd_rows_f32_k(const PoissonPlan &pp, const Chan
     const int j0 = 2 * pair, j1 = j0 + 1;
     const bool live = j0 < pp.n, two = j1 < pp.n;
     const int nxp = c.nxp;
-    const float *r0 = pp.rhsf + (size_t)(j0 + 1) * nxp + t, *r1 = pp.rhsf + (size_t)(j1 + 1) * nxp + t;
+    // 32-bit offsets from the planes' base pointers (a plane is below 2^32
+    // elements: one channel's planes fit device memory)
+    const unsigned r0 = (unsigned)(j0 + 1) * (unsigned)nxp + (unsigned)t, r1 = r0 + (unsigned)nxp;
     const double k0 = live ? rhs_row_constant(pp, c, j0 + 1) : 0.0, k1 = two ? rhs_row_constant(pp, c, j1 + 1) : 0.0;
     const bool exact = *pp.rowmean_ok == 0;  // the same for every block of the launch
     // value - offset = rhsf + (row constant - offset)
@@ -434,7 +436,8 @@ __device__ __forceinline__ void fwd_rows_f32_k(const PoissonPlan &pp, const Chan
     float2 x[16];
 #pragma unroll
     for (int v = 0; v < 16; ++v) {
-        const float f0 = live ? __ldg(r0 + v * T) : 0.0f, f1 = two ? __ldg(r1 + v * T) : 0.0f;
+        const float f0 = live ? __ldg(pp.rhsf + (r0 + (unsigned)(v * T))) : 0.0f,
+                    f1 = two ? __ldg(pp.rhsf + (r1 + (unsigned)(v * T))) : 0.0f;
         a0 += (double)f0;
         a1 += (double)f1;
         x[v] = make_float2((float)((double)f0 + d0), (float)((double)f1 + d1));
@@ -446,8 +449,8 @@ __device__ __forceinline__ void fwd_rows_f32_k(const PoissonPlan &pp, const Chan
         d1 = k1 - a1 / (double)N;
 #pragma unroll
         for (int v = 0; v < 16; ++v)
-            x[v] = make_float2(live ? (float)((double)__ldg(r0 + v * T) + d0) : 0.0f,
-                               two ? (float)((double)__ldg(r1 + v * T) + d1) : 0.0f);
+            x[v] = make_float2(live ? (float)((double)__ldg(pp.rhsf + (r0 + (unsigned)(v * T))) + d0) : 0.0f,
+                               two ? (float)((double)__ldg(pp.rhsf + (r1 + (unsigned)(v * T))) + d1) : 0.0f);
     }
     if (t == 0 && live) {
         pp.spec[(size_t)j0 * pp.mp] = make_double2(a0, 0.0);
@@ -461,12 +464,12 @@ __device__ __forceinline__ void fwd_rows_f32_k(const PoissonPlan &pp, const Chan
     __syncthreads();
     fft32::fwd_rest<K, 2>(s, t, p, pp.twf);
     if (!live) return;
-    float2 *s0 = pp.specf + (size_t)j0 * pp.mp, *s1 = pp.specf + (size_t)j1 * pp.mp;
+    const unsigned q0 = (unsigned)j0 * (unsigned)pp.mp, q1 = q0 + (unsigned)pp.mp;
     for (int m = t; m <= N / 2; m += T) {
         if (m == 0) continue;
         const float2 a = s[fft32::swz_base(brev(m, K), p)], b = cconj(s[fft32::swz_base(brev(N - m, K), p)]);
-        s0[m] = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y + b.y));
-        if (two) s1[m] = make_float2(0.5f * (a.y - b.y), -0.5f * (a.x - b.x));
+        pp.specf[q0 + (unsigned)m] = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y + b.y));
+        if (two) pp.specf[q1 + (unsigned)m] = make_float2(0.5f * (a.y - b.y), -0.5f * (a.x - b.x));
     }
 }
 
@@ -508,7 +511,8 @@ __device__ __forceinline__ void inv_rows_f32_k(const PoissonPlan &pp, const Chan
     const int nxp = c.nxp;
     constexpr int per = BLOCK / T;
     write_walls_f32(pp, c, psi, write_f64, pair_base / per, ((pp.n + 1) / 2 + per - 1) / per, BLOCK);
-    const float2 *s0 = pp.specf + (size_t)j0 * pp.mp, *s1 = pp.specf + (size_t)j1 * pp.mp;
+    // 32-bit offsets from the planes' base pointers (as in fwd_rows_f32_k)
+    const unsigned q0 = (unsigned)j0 * (unsigned)pp.mp, q1 = q0 + (unsigned)pp.mp;
     // modes m = t + i T (i < 8) and, for t = 0, m = N/2: all loads first
     const float2 zero = make_float2(0.0f, 0.0f);
     float2 a[9], b[9];
@@ -516,8 +520,8 @@ __device__ __forceinline__ void inv_rows_f32_k(const PoissonPlan &pp, const Chan
     for (int i = 0; i < 9; ++i) {
         const int m = t + i * T;
         const bool in = i < 8 || t == 0;
-        a[i] = (live && in && m) ? s0[m] : zero;
-        b[i] = (two && in && m) ? s1[m] : zero;
+        a[i] = (live && in && m) ? pp.specf[q0 + (unsigned)m] : zero;
+        b[i] = (two && in && m) ? pp.specf[q1 + (unsigned)m] : zero;
     }
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
@@ -542,16 +546,16 @@ __device__ __forceinline__ void inv_rows_f32_k(const PoissonPlan &pp, const Chan
             pp.psim[j0 + 1] = mean0;
             if (two) pp.psim[j1 + 1] = mean1;
         }
-        float *f0 = pp.psif + (size_t)(j0 + 1) * nxp + t, *f1 = pp.psif + (size_t)(j1 + 1) * nxp + t;
-        double *p0 = psi + (size_t)(j0 + 1) * nxp + t, *p1 = psi + (size_t)(j1 + 1) * nxp + t;
+        const unsigned o0 = (unsigned)(j0 + 1) * (unsigned)nxp + (unsigned)t, o1 = o0 + (unsigned)nxp;
 #pragma unroll
         for (int v = 0; v < 16; ++v) {
-            const float q0 = x[v].x * invf, q1 = x[v].y * invf;
-            st_field_f(f0 + v * T, q0, pp.keep_l2);
-            if (two) st_field_f(f1 + v * T, q1, pp.keep_l2);
+            const float y0 = x[v].x * invf, y1 = x[v].y * invf;
+            const unsigned dv = (unsigned)(v * T);
+            st_field_f(pp.psif + (o0 + dv), y0, pp.keep_l2);
+            if (two) st_field_f(pp.psif + (o1 + dv), y1, pp.keep_l2);
             if (write_f64) {
-                p0[v * T] = mean0 + (double)q0;
-                if (two) p1[v * T] = mean1 + (double)q1;
+                psi[o0 + dv] = mean0 + (double)y0;
+                if (two) psi[o1 + dv] = mean1 + (double)y1;
             }
         }
     }
