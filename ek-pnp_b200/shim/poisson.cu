@@ -11,9 +11,11 @@
 // frees four buffers per call, poisson.cu:182-207).
 //
 // The reference's helpers of its cuFFT pipeline (extension, derivative,
-// extract, poisson_phi: odd-extended complex arrays and the dead Jacobi
-// iteration) have no counterpart: the library's solve never forms the
-// odd-extended array.  A caller that used them directly calls fast_Poisson.
+// extract: odd-extended complex arrays) have no counterpart: the library's
+// solve never forms the odd-extended array.  A caller that used them
+// directly calls fast_Poisson.  poisson_phi, the reference's iterative
+// solver (poisson.cu:35-130, not called by main.cu), runs the library's
+// grid relaxation (ek_poisson_jacobi).
 #ifndef EKPNP_SHIM_POISSON_CU
 #define EKPNP_SHIM_POISSON_CU
 
@@ -35,6 +37,49 @@ __host__ void fast_Poisson(double *charge_d, double *T_d, double *kx_, double *k
     check(ek_get_fields_device(ctx(), nullptr, nullptr, nullptr, nullptr, nullptr, phi_gpu, Ex_gpu, Ey_gpu),
           "ek_get_fields_device");
     check(ek_sync(ctx()), "ek_sync");
+}
+
+// c+ = rho_e / f_charge, c- = 0: the library's right-hand side
+// -f_charge (c+ - c-) / eps is then the reference's -rho_e / eps.
+__global__ void ekshim_charge_to_cp(const double *rho_e, double *cp, double *cn, double inv_f, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        cp[i] = rho_e[i] * inv_f;
+        cn[i] = 0.0;
+    }
+}
+
+// poisson_phi (poisson.cu:35-73): psi for the net charge density in
+// charge_d by grid relaxation from the potential in phi_d, walls at
+// voltage / voltage2, until the largest change of a sweep is below 1e-9 or
+// 1e6 sweeps, then psi into phi_d.  The library's sweeps read one buffer and
+// write another, so unlike the reference's in-place update the result does
+// not depend on the block schedule; the change is measured every 100 sweeps
+// instead of after every one.
+__host__ void poisson_phi(double *charge_d, double *phi_d) {
+    using namespace ekshim;
+    const int n = (int)(NX * NY);
+    double *cp = nullptr, *cn = nullptr;
+    checkCudaErrors(cudaMalloc(&cp, mem_size_scalar));
+    checkCudaErrors(cudaMalloc(&cn, mem_size_scalar));
+    ekshim_charge_to_cp<<<(n + 255) / 256, 256>>>(charge_d, cp, cn, 1.0 / from_symbol(convertCtoCharge), n);
+    checkCudaErrors(cudaGetLastError());
+    checkCudaErrors(cudaDeviceSynchronize());
+    check(ek_set_fields_device(ctx(), nullptr, nullptr, nullptr, cp, cn, phi_d, nullptr, nullptr),
+          "ek_set_fields_device");
+    int32_t sweeps = 0;
+    double change = 0.0;
+    const int32_t max_sweeps = 1000000;
+    check(ek_poisson_jacobi(ctx(), max_sweeps, 1.0e-9, 1.0, 100, &sweeps, &change), "ek_poisson_jacobi");
+    check(ek_get_fields_device(ctx(), nullptr, nullptr, nullptr, nullptr, nullptr, phi_d, nullptr, nullptr),
+          "ek_get_fields_device");
+    check(ek_sync(ctx()), "ek_sync");
+    checkCudaErrors(cudaFree(cp));
+    checkCudaErrors(cudaFree(cn));
+    if (!(change < 1.0e-9)) {
+        printf("Poisson solver did not converge!\n");
+        printf("Residual = %g\n", change);
+    }
 }
 
 // E = -grad psi with the reference's stencil (gpu_efield + gpu_bc,
