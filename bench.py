@@ -341,7 +341,7 @@ def run_batch(args, d):
             "config": {"workload": args.workload, "channels": count, "nodes": total_nodes,
                        "nodes_rank0": nn,
                        "storage": args.storage + "-shifted",
-                       "block_shape": dict(zip(("threads", "tile_width", "blocks_per_sm", "pipelined"), Batch.shapes()[chosen])),
+                       "block_shape": dict(zip(("threads", "tile_width", "blocks_per_sm"), Batch.shapes()[chosen])),
                        "autotune_ms_per_step": {"x".join(map(str, sh)): round(m, 4)
                                                 for sh, m in zip(Batch.shapes(), tune_ms)},
                        "cycle": 200, "graph": graph,
@@ -398,7 +398,7 @@ def run_batch_steady(args, d):
         "data": "synthetic (seeded channel draw and noisy cold start from the same stream)",
         "config": {"workload": f"batch-{count}-to-steady", "channels": count, "nodes": nodes,
                    "storage": args.storage + "-shifted", "tol": 1e-8, "cap_steps": cap, "check_every": check,
-                   "block_shape": dict(zip(("threads", "tile_width", "blocks_per_sm", "pipelined"), Batch.shapes()[chosen])),
+                   "block_shape": dict(zip(("threads", "tile_width", "blocks_per_sm"), Batch.shapes()[chosen])),
                    "cycle": 200, "graph": True, "freeze_converged": True},
         "wall_s": info["wall_s"], "node_steps": int(info["node_steps"]),
         "converged": int(ok.sum()), "diverged": int(np.sum(info["diverged"])),
@@ -713,7 +713,7 @@ def main():
     ap.add_argument("--to-steady", action="store_true",
                     help="with --batch: run the 512 channels from their cold start to residual < 1e-8")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--lbm-kernel", choices=("auto", "plain", "tma", "rows"), default="auto",
+    ap.add_argument("--lbm-kernel", choices=("auto", "plain", "tma"), default="auto",
                     help="form of the shifted-storage LBM kernel (bit-identical forms)")
     args = ap.parse_args()
     if args.warmup < 3:

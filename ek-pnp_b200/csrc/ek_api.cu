@@ -13,7 +13,6 @@
 #include <cstring>
 #include <map>
 #include <string>
-#include <thread>
 #include <utility>
 #include <vector>
 
@@ -350,47 +349,6 @@ int split_if_stale(ek_ctx *c) {
     return EK_OK;
 }
 
-// Discrete 1D Poisson-Boltzmann equation down one column (rows 1..ny-2):
-//   (psi_{j-1} - 2 psi_j + psi_{j+1})/dy^2 + g (exp(-a psi_j) - exp(a psi_j)) = 0
-// with psi_0 = zl, psi_{ny-1} = zh, g = f_charge c0/eps, a = e/kT.  Damped
-// Newton from the linear profile; each step changes a*psi by at most 1.
-bool pb_column(int ny, double dy, double g, double a, double zl, double zh, std::vector<double> &psi) {
-    psi.assign(ny, 0.0);
-    for (int j = 0; j < ny; ++j) psi[j] = zl + (zh - zl) * (double)j / (double)(ny - 1);
-    const int n = ny - 2;
-    const double inv = 1.0 / (dy * dy);
-    std::vector<double> rhs(n), diag(n), cp(n), dp(n);
-    const double scale = std::max({std::fabs(zl), std::fabs(zh), 1.0});
-    int polish = -1;  // full Newton steps left once the update is small
-    for (int it = 0; it < 500; ++it) {
-        double gmax = 0.0;
-        for (int j = 0; j < n; ++j) {
-            const double v = psi[j + 1], em = std::exp(-a * v), ep = std::exp(a * v);
-            const double G = (psi[j] - 2.0 * v + psi[j + 2]) * inv + g * (em - ep);
-            rhs[j] = -G;
-            diag[j] = -2.0 * inv - g * a * (em + ep);
-            gmax = std::max(gmax, std::fabs(G));
-        }
-        // Thomas solve of J delta = -G (off-diagonals inv)
-        cp[0] = inv / diag[0];
-        dp[0] = rhs[0] / diag[0];
-        for (int j = 1; j < n; ++j) {
-            const double den = diag[j] - inv * cp[j - 1];
-            cp[j] = inv / den;
-            dp[j] = (rhs[j] - inv * dp[j - 1]) / den;
-        }
-        for (int j = n - 2; j >= 0; --j) dp[j] -= cp[j] * dp[j + 1];
-        double dmax = 0.0;
-        for (int j = 0; j < n; ++j) dmax = std::max(dmax, std::fabs(a * dp[j]));
-        const double damp = dmax > 1.0 ? 1.0 / dmax : 1.0;
-        for (int j = 0; j < n; ++j) psi[j + 1] += damp * dp[j];
-        (void)gmax;
-        // quadratic convergence: two more full steps after |a delta| < 1e-9 reach rounding
-        if (polish < 0 && damp == 1.0 && dmax < 1e-9 * scale) polish = 2;
-        if (polish >= 0 && polish-- == 0) return true;
-    }
-    return false;
-}
 
 }  // namespace
 
@@ -734,38 +692,43 @@ int ek_init_poisson_boltzmann(ek_ctx *c, int32_t method, int32_t iterations, dou
     if (method != EK_PB_NEWTON) return fail(EK_ERR_INVALID, "unknown Poisson-Boltzmann method");
     const int nx = p.nx, ny = p.ny;
     const double g = p.f_charge * p.c0 / p.eps;
-    // one Newton solve per distinct pair of wall potentials
-    std::map<std::pair<double, double>, std::vector<double>> prof;
-    for (int x = 0; x < nx; ++x) prof[{c->wall_host[x], c->wall_host[nx + x]}];
-    std::vector<std::pair<const std::pair<double, double>, std::vector<double>> *> work;
-    for (auto &kv : prof) work.push_back(&kv);
-    std::vector<int> ok(work.size(), 1);
-    const unsigned nt = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), (unsigned)work.size()));
-    std::vector<std::thread> pool;
-    for (unsigned t = 0; t < nt; ++t)
-        pool.emplace_back([&, t] {
-            for (size_t i = t; i < work.size(); i += nt)
-                ok[i] = pb_column(ny, p.dy, g, e_kt, work[i]->first.first, work[i]->first.second, work[i]->second);
-        });
-    for (auto &th : pool) th.join();
+    // one Newton solve per distinct pair of wall potentials, on the device
+    std::map<std::pair<double, double>, int> index;
+    std::vector<double2> walls;
+    std::vector<int> colmap(nx);
+    for (int x = 0; x < nx; ++x) {
+        const std::pair<double, double> key{c->wall_host[x], c->wall_host[nx + x]};
+        auto it = index.find(key);
+        if (it == index.end()) {
+            it = index.emplace(key, (int)walls.size()).first;
+            walls.push_back(make_double2(key.first, key.second));
+        }
+        colmap[x] = it->second;
+    }
+    const int ncol = (int)walls.size();
+    // one allocation: the 16-byte wall pairs first, then the three ny x ncol
+    // columns of doubles, then the ints
+    const size_t bytes = (size_t)ncol * sizeof(double2) + 3 * (size_t)ny * ncol * sizeof(double) +
+                         (size_t)(nx + ncol) * sizeof(int);
+    char *scratch = nullptr;
+    EK_CUDA(cudaMalloc(&scratch, bytes), "Newton PB scratch");
+    double2 *dwalls = (double2 *)scratch;
+    double *psi = (double *)(dwalls + ncol), *cpv = psi + (size_t)ny * ncol, *dpv = cpv + (size_t)ny * ncol;
+    int *dmap = (int *)(dpv + (size_t)ny * ncol), *dok = dmap + nx;
+    std::vector<int> ok(ncol, 0);
+    cudaError_t e = cudaMemcpyAsync(dwalls, walls.data(), walls.size() * sizeof(double2), cudaMemcpyHostToDevice,
+                                    c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dmap, colmap.data(), (size_t)nx * sizeof(int), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess)
+        e = launch_pb_newton(c->chan, p.dy, g, e_kt, dwalls, ncol, psi, cpv, dpv, dok, dmap, c->fields, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(ok.data(), dok, (size_t)ncol * sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(scratch);
+    EK_CUDA(e, "Newton PB");
     for (int v : ok)
         if (!v) return fail(EK_ERR_INVALID, "Poisson-Boltzmann Newton iteration did not converge");
-    std::vector<double> rho((size_t)nx * ny, p.rho0), zero((size_t)nx * ny, 0.0), psi((size_t)nx * ny),
-        cpv((size_t)nx * ny), cnv((size_t)nx * ny);
-    for (int x = 0; x < nx; ++x) {
-        const std::vector<double> &col = prof[{c->wall_host[x], c->wall_host[nx + x]}];
-        for (int y = 0; y < ny; ++y) {
-            const size_t k = (size_t)y * nx + x;
-            psi[k] = col[y];
-            cpv[k] = p.c0 * std::exp(-e_kt * col[y]);
-            cnv[k] = p.c0 * std::exp(e_kt * col[y]);
-        }
-    }
-    const double *src[F_RHS] = {rho.data(), zero.data(), zero.data(), cpv.data(), cnv.data(), psi.data(), nullptr, nullptr};
-    for (int k = 0; k < F_RHS; ++k) {
-        int rc = copy_in(c, k, src[k]);
-        if (rc != EK_OK) return rc;
-    }
     EK_CUDA(cudaStreamSynchronize(c->stream), "PB upload");
     c->explicit_e_once = false;
     c->e_stale = true;

@@ -723,6 +723,33 @@ int ek_batch_resync(ek_batch *b) {
 // batch's current buffer parity (an even number of batch steps since they
 // were frozen).  Launches per step stay the same; the work shrinks to the
 // active channels.
+int ek_batch_restart(ek_batch *b, const uint8_t *mask) {
+    if (!b || !mask) return ek::ctx_fail(EK_ERR_INVALID, "null argument");
+    EK_BCUDA(cudaStreamSynchronize(b->stream), "batch sync");
+    bool any = false;
+    for (size_t i = 0; i < b->ch.size(); ++i) {
+        if (!mask[i]) continue;
+        ek_ctx *c = b->ch[i];
+        if (!c->initialised) return ek::ctx_fail(EK_ERR_INVALID, "call ek_batch_init_equilibrium first");
+        // equilibrium populations of the channel's loaded fields, written to
+        // the buffer the batch steps from next; that step pulls them
+        c->cur = b->cur;
+        const int rc = ek_init_equilibrium(c);
+        if (rc != EK_OK) return rc;
+        EK_BCUDA(cudaStreamSynchronize(c->stream), "restart sync");
+        c->state_pre = b->state_pre;
+        c->explicit_e_once = b->explicit_e_once;
+        b->ch_steps[i] = 0;
+        c->steps = 0;
+        b->active[i] = 1;
+        any = true;
+    }
+    if (!any) return EK_OK;
+    int rc = build_tables(b);  // reference rows and exponents of the restarted channels changed
+    if (rc == EK_OK) rc = build_tiles(b, b->shape);
+    return rc;
+}
+
 int ek_batch_set_active(ek_batch *b, const uint8_t *mask) {
     if (!b || !mask) return ek::ctx_fail(EK_ERR_INVALID, "null argument");
     EK_BCUDA(cudaStreamSynchronize(b->stream), "batch sync");

@@ -153,6 +153,12 @@ cudaError_t launch_rhs_from_moments_f64(const Chan &c, double *fields, cudaStrea
 cudaError_t launch_pb_fill(const Chan &c, double *fields, double *psi_old, cudaStream_t s);
 cudaError_t launch_pb_conc(const Chan &c, double e_kt, double *fields, cudaStream_t s);
 cudaError_t launch_pb_relax(const Chan &c, double omega, double *fields, double *psi_old, cudaStream_t s);
+// Newton Poisson-Boltzmann start: ncol columns (walls[q] = {zeta_lo, zeta_hi})
+// solved on the device (psi, cp, dp: ny x ncol scratch, ok: ncol flags), then
+// the fields of every node from its column colmap[x].
+cudaError_t launch_pb_newton(const Chan &c, double dy, double g, double a, const double2 *walls, int ncol,
+                             double *psi, double *cp, double *dp, int *ok, const int *colmap, double *fields,
+                             cudaStream_t s);
 
 // ---- shifted-storage forms (ek_lbm_f32.cu); storage = EK_STORE_F32 or _F16 ----
 // sbuf: index (0/1) of the population buffer that src is (it names the wall

@@ -142,37 +142,58 @@ __device__ __forceinline__ void efield_at(const double *__restrict__ psi, const 
     *ey = 0.5 * (__ldg(psi + (size_t)(yc - 1) * c.nxp + x) - __ldg(psi + (size_t)(yc + 1) * c.nxp + x)) / c.dy;
 }
 
-template <bool FIRST, bool EXPLICIT_E, bool MOMENTS, typename I>
-__global__ void __launch_bounds__(TPB)
-step_f64(const Chan c, const double *__restrict__ src, double *__restrict__ dst,
-         double *__restrict__ fields) {
-    const int x = blockIdx.x * TPB + threadIdx.x;
-    const int y = blockIdx.y;
-    if (x >= c.nx) return;
+// The raw populations of node (x, y) as stored: FIRST -> its own values;
+// otherwise the fluid pulled from the neighbours and the ions pulled
+// (interior rows) or the node's own values (wall rows, reflected by node_f64).
+template <bool FIRST, typename I>
+__device__ __forceinline__ void gather_f64(const Chan &c, const double *__restrict__ src, int x, int y, double ft[9],
+                                           double ht[9], double tt[9]) {
     const I pl = (I)c.plane;
     const int nxp = c.nxp;
     const I o = (I)y * (I)nxp + (I)x;
-    const bool lo = y == 0, hi = y == c.ny - 1;
     const int xm = x == 0 ? c.nx - 1 : x - 1, xp = x + 1 == c.nx ? 0 : x + 1;
     const int ym = y == 0 ? c.ny - 1 : y - 1, yp = y + 1 == c.ny ? 0 : y + 1;
     const double *sf = src, *sh = src + 9 * pl, *st = src + 18 * pl;
-
-    double ft[9], ht[9], tt[9];
     if (FIRST) {
         own9(sf, pl, o, ft);
         own9(sh, pl, o, ht);
         own9(st, pl, o, tt);
     } else {
         pull9(sf, pl, nxp, x, y, xm, xp, ym, yp, ft);
-        if (lo || hi) {
-            double q[9];
-            own9(sh, pl, o, q);
-            ion_wall(q, lo ? c.cplo[x] : c.cphi[x], ht);
-            own9(st, pl, o, q);
-            ion_wall(q, lo ? c.cnlo[x] : c.cnhi[x], tt);
+        if (y == 0 || y == c.ny - 1) {
+            own9(sh, pl, o, ht);
+            own9(st, pl, o, tt);
         } else {
             pull9(sh, pl, nxp, x, y, xm, xp, ym, yp, ht);
             pull9(st, pl, nxp, x, y, xm, xp, ym, yp, tt);
+        }
+    }
+}
+
+// The update of node (x, y) from its raw populations (gather_f64): ion
+// anti-bounce-back at the walls, moments, E, force, right-hand side,
+// equilibria, Guo source, TRT and the stores.  src is read only for the lower
+// wall's row-1 pull.
+template <bool FIRST, bool EXPLICIT_E, bool MOMENTS, typename I>
+__device__ __forceinline__ void node_f64(const Chan &c, double ft[9], double ht_raw[9], double tt_raw[9],
+                                         const double *__restrict__ src, double *__restrict__ dst,
+                                         double *__restrict__ fields, int x, int y) {
+    const I pl = (I)c.plane;
+    const int nxp = c.nxp;
+    const I o = (I)y * (I)nxp + (I)x;
+    const bool lo = y == 0, hi = y == c.ny - 1;
+    const int xm = x == 0 ? c.nx - 1 : x - 1, xp = x + 1 == c.nx ? 0 : x + 1;
+    const double *sf = src;
+
+    double ht[9], tt[9];
+    if (!FIRST && (lo || hi)) {
+        ion_wall(ht_raw, lo ? c.cplo[x] : c.cphi[x], ht);
+        ion_wall(tt_raw, lo ? c.cnlo[x] : c.cnhi[x], tt);
+    } else {
+#pragma unroll
+        for (int d = 0; d < 9; ++d) {
+            ht[d] = ht_raw[d];
+            tt[d] = tt_raw[d];
         }
     }
 
@@ -281,6 +302,18 @@ step_f64(const Chan c, const double *__restrict__ src, double *__restrict__ dst,
     relax(ft, e, c.r.wp, c.r.wm, out);
 #pragma unroll
     for (int d = 0; d < 9; ++d) df[d * pl + o] = out[d] + dt * src9[d];
+}
+
+template <bool FIRST, bool EXPLICIT_E, bool MOMENTS, typename I>
+__global__ void __launch_bounds__(TPB)
+step_f64(const Chan c, const double *__restrict__ src, double *__restrict__ dst,
+         double *__restrict__ fields) {
+    const int x = blockIdx.x * TPB + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= c.nx) return;
+    double ft[9], ht[9], tt[9];
+    gather_f64<FIRST, I>(c, src, x, y, ft, ht, tt);
+    node_f64<FIRST, EXPLICIT_E, MOMENTS, I>(c, ft, ht, tt, src, dst, fields, x, y);
 }
 
 __global__ void rates_kernel(ek_params p, Rates *out) {

@@ -114,6 +114,7 @@ _SIGS = {
     "ek_batch_residual": ([ctypes.c_void_p, ctypes.c_int32, _dp, _dp], ctypes.c_int),
     "ek_batch_set_active": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "ek_batch_resync": ([ctypes.c_void_p], ctypes.c_int),
+    "ek_batch_restart": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "ek_batch_active": ([ctypes.c_void_p, ctypes.c_void_p, _P(ctypes.c_int64)], ctypes.c_int),
     "ek_write_restart": ([ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_double] + [_dp] * 8, ctypes.c_int),
     "ek_read_restart": ([ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, _dp] + [_dp] * 8, ctypes.c_int),

@@ -125,6 +125,14 @@ class Batch:
         """Adopt the channels' current states (after Channel.tile_x)."""
         check(lib().ek_batch_resync(self._h))
 
+    def restart(self, mask):
+        """Restart the masked channels in place from the fields loaded through
+        their own handles (Channel.set_fields); the others step on untouched."""
+        m = np.ascontiguousarray(np.asarray(mask, dtype=bool).astype(np.uint8))
+        if m.shape != (len(self.channels),):
+            raise ValueError("one flag per channel")
+        check(lib().ek_batch_restart(self._h, ctypes.c_void_p(m.ctypes.data)))
+
     def set_active(self, mask):
         """Freeze (False) or step (True) each channel."""
         m = np.ascontiguousarray(np.asarray(mask, dtype=bool).astype(np.uint8))

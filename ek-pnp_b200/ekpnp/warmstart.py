@@ -162,7 +162,12 @@ def physics_start(batch, specs):
         ch.set_fields(**profile_fields(s, physics_profiles(s), nx=ch.nx))
 
 
-def run_to_steady(batch, tol=1e-8, check=1000, max_steps=200_000, judge=None, freeze=True):
+# Residual recorded for a channel at the check where it is restarted and the
+# one after (finite: the channel is neither converged nor diverged there).
+UNJUDGED = 1e300
+
+
+def run_to_steady(batch, tol=1e-8, check=1000, max_steps=200_000, judge=None, freeze=True, restart=None):
     """Step the batch until every channel has residual < tol (checked every
     `check` steps, an even number) or diverged, or max_steps.  With freeze,
     channels stop stepping once converged or diverged (and, with judge, once
@@ -171,11 +176,18 @@ def run_to_steady(batch, tol=1e-8, check=1000, max_steps=200_000, judge=None, fr
     per check; frozen channels repeat their last value), the wall time in
     seconds (host clock, checks included) and the node updates of the stepping
     channels (node_steps).  judge=(k1, k2): also return the channels whose
-    worst residual rose from check k1 to check k2."""
+    worst residual rose from check k1 to check k2.  restart(indices): with
+    judge, such channels (and those that go non-finite first) are handed to
+    restart -- which gives them a new start in place (Batch.restart) -- once
+    each, instead of being frozen; they step on with the others, their steps
+    to steady count from the batch's start, and the check right after a
+    restart (which compares with the state before it) is not judged."""
     n = len(batch)
     steps_to = np.full(n, -1, dtype=np.int64)
     hist = []
     done = np.zeros(n, bool)
+    restarted = np.zeros(n, bool)
+    fresh = np.zeros(n, bool)  # restarted at the previous check
     last = np.full(n, np.inf)
     node_steps = 0
     batch.sync()
@@ -186,7 +198,18 @@ def run_to_steady(batch, tol=1e-8, check=1000, max_steps=200_000, judge=None, fr
         node_steps += batch.active[1] * k
         batch.step(k)
         r = batch.residual(check)[:, 4]
+        r = np.where(fresh, UNJUDGED, r)
+        fresh[:] = False
         r = np.where(done, last, r)
+        if restart is not None and judge is not None:
+            cand = ~restarted & ~done & ~np.isfinite(r)
+            if len(hist) + 1 > judge[1]:
+                cand |= ~restarted & ~done & rising_channels(np.array(hist + [r]), *judge)
+            if cand.any():
+                restart(np.nonzero(cand)[0])
+                restarted |= cand
+                fresh |= cand
+                r = np.where(cand, UNJUDGED, r)
         last = r
         hist.append(r)
         ok = np.isfinite(r)
@@ -196,7 +219,7 @@ def run_to_steady(batch, tol=1e-8, check=1000, max_steps=200_000, judge=None, fr
             break
         if freeze:
             stop = (steps_to >= 0) | ~ok
-            if judge is not None and len(hist) > judge[1]:
+            if judge is not None and restart is None and len(hist) > judge[1]:
                 stop |= rising_channels(np.array(hist), *judge)
             if np.any(stop & ~done):
                 done |= stop
@@ -204,8 +227,14 @@ def run_to_steady(batch, tol=1e-8, check=1000, max_steps=200_000, judge=None, fr
     wall = time.perf_counter() - t0
     hist = np.array(hist)
     diverged = ~np.isfinite(hist[-1]) if len(hist) else np.zeros(n, bool)
-    rising = None if judge is None else rising_channels(hist, *judge)
-    return dict(steps=steps_to, diverged=diverged, history=hist, wall_s=wall, rising=rising, node_steps=node_steps)
+    if judge is None:
+        rising = None
+    elif restart is not None:
+        rising = restarted
+    else:
+        rising = rising_channels(hist, *judge)
+    return dict(steps=steps_to, diverged=diverged, history=hist, wall_s=wall, rising=rising, node_steps=node_steps,
+                restarted=restarted)
 
 
 def rising_channels(hist, k1, k2):
@@ -300,28 +329,33 @@ class Surrogate:
 def start_run(specs, fields, tol=1e-8, check=1000, max_steps=200_000, storage=STORE_F32, cycle=200, judge=None):
     """Run the channels from the given start fields to steady state.  With
     judge=(k1, k2) the channels whose residual rises between checks k1 and k2,
-    or that diverge, are re-run from the uniform cold start (their steps then
-    count from that start; the wall time covers both runs)."""
+    or that diverge, are restarted in place from the uniform cold start and
+    step on with the others (their steps count from the batch's start; the
+    wall time covers the whole batch)."""
     t0 = time.perf_counter()
     with Batch([spec_params(s, storage) for s in specs]) as b:
         for ch, f in zip(b, fields):
             ch.set_fields(**f)
         b.set_cycle(cycle)
         b.init_equilibrium()
-        info = run_to_steady(b, tol=tol, check=check, max_steps=max_steps, judge=judge)
+        info = run_to_steady(b, tol=tol, check=check, max_steps=max_steps, judge=judge,
+                             restart=None if judge is None else cold_restart(b, specs))
         final = [profiles(ch) for ch in b]
-    steps = info["steps"].copy()
-    fallback = np.nonzero(info["rising"])[0] if judge is not None else np.zeros(0, dtype=np.int64)
-    cold = None
-    if len(fallback):
-        sub = [specs[i] for i in fallback]
-        cold = start_run(sub, [cold_state(s) for s in sub], tol=tol, check=check, max_steps=max_steps,
-                         storage=storage, cycle=cycle)
-        steps[fallback] = cold["steps"]
-        for j, i in enumerate(fallback):
-            final[i] = cold["final"][j]
-    return dict(steps=steps, wall_s=time.perf_counter() - t0, first=info, fallback=fallback, cold=cold,
+    fallback = np.nonzero(info["restarted"])[0]
+    return dict(steps=info["steps"].copy(), wall_s=time.perf_counter() - t0, first=info, fallback=fallback,
                 final=final, diverged=info["diverged"])
+
+
+def cold_restart(batch, specs):
+    """A restart callback for run_to_steady: the channels' uniform cold start,
+    loaded and restarted in place."""
+    def restart(idx):
+        mask = np.zeros(len(batch), bool)
+        for i in idx:
+            batch[i].set_fields(**cold_state(specs[i]))
+            mask[i] = True
+        batch.restart(mask)
+    return restart
 
 
 def warm_start_run(surrogate, specs, judge=(1, 3), **kw):
@@ -354,7 +388,7 @@ def xreduced_start_run(specs, start="cold", surrogate=None, narrow_nx=16, tol=1e
     make the steady state independent of x, so each channel first relaxes on
     narrow_nx columns (start "cold": the uniform cold start; "surrogate": the
     network's start, judged as in warm_start_run with the cold start as
-    fallback; "physics": the Poisson-Boltzmann/electro-osmotic start without
+    in-place fallback; "physics": the Poisson-Boltzmann/electro-osmotic start without
     the network), then its relaxed state is tiled along x into the full channel
     (ek_tile_x) and the full batch steps to the same residual.  Steps and wall
     time count both stages (inference, both batches' set-up and the copies
@@ -385,22 +419,10 @@ def xreduced_start_run(specs, start="cold", surrogate=None, narrow_nx=16, tol=1e
             ch.set_fields(**f)
         nb.set_cycle(cycle)
         nb.init_equilibrium()
-        narrow = run_to_steady(nb, judge=judge, **nkw)
+        narrow = run_to_steady(nb, judge=judge, restart=None if judge is None else cold_restart(nb, nspecs), **nkw)
         src = list(nb)
         nsteps = narrow["steps"].copy()
-        fallback = np.nonzero(narrow["rising"])[0] if judge is not None else np.zeros(0, dtype=np.int64)
-        if len(fallback):
-            sub = [nspecs[i] for i in fallback]
-            fb = Batch([spec_params(s, storage) for s in sub])
-            batches.append(fb)
-            for ch, s in zip(fb, sub):
-                ch.set_fields(**cold_state(s))
-            fb.set_cycle(cycle)
-            fb.init_equilibrium()
-            again = run_to_steady(fb, **nkw)
-            for j, i in enumerate(fallback):
-                src[i] = fb[j]
-                nsteps[i] = again["steps"][j]
+        fallback = np.nonzero(narrow["restarted"])[0]
         t_narrow = time.perf_counter() - t0
         with Batch([spec_params(s, storage) for s in specs]) as wb:
             wb.set_cycle(cycle)

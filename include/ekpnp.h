@@ -155,8 +155,9 @@ int ek_set_wall_profile(ek_ctx *ctx, const double *zeta_lo, const double *zeta_h
  *     converges only for weak coupling (roughly kappa*H below 10 at |zeta| = 2).
  *   method EK_PB_NEWTON: damped Newton iteration of the discrete 1D
  *     Poisson-Boltzmann equation down every x-column (rows 1..ny-2, Dirichlet
- *     wall values), iterations/omega ignored.  Exact for walls uniform in x,
- *     the column-local solution otherwise.
+ *     wall values), iterations/omega ignored, on the device (one thread per
+ *     distinct pair of wall potentials, 3 ny doubles of scratch each).  Exact
+ *     for walls uniform in x, the column-local solution otherwise.
  * Follow with ek_init_equilibrium (optionally after perturbing the fields). */
 enum { EK_PB_REFERENCE = 0, EK_PB_NEWTON = 1 };
 int ek_init_poisson_boltzmann(ek_ctx *ctx, int32_t method, int32_t iterations,
@@ -194,8 +195,8 @@ int ek_set_rebase_interval(ek_ctx *ctx, int32_t steps);
  * shifted-storage LBM kernel: 0 = automatic (currently the plain form, the
  * faster one on B200), 1 = plain per-node loads, 2 = TMA-fed pipeline
  * (producer warp + mbarrier ring of tensor copies).  Both forms give
- * bit-identical results.  Returns EK_ERR_UNSUPPORTED for a form that this
- * context cannot run. */
+ * bit-identical results.
+ * Returns EK_ERR_UNSUPPORTED for a form that this context cannot run. */
 enum { EK_OPT_LBM_KERNEL = 1, EK_OPT_POISSON = 2, EK_OPT_LAST_STEP_MOMENTS = 3, EK_OPT_WAIT_CYCLES = 4 };
 /* EK_OPT_POISSON selects the arithmetic of the Poisson solve (ek_step and
  * ek_poisson): 0 = automatic (the FP32 form for FP32/FP16 storage where it
@@ -392,6 +393,16 @@ int ek_batch_set_active(ek_batch *b, const uint8_t *mask);
  * handles (ek_tile_x): all channels must be initialised and at one step
  * parity and state; the batch steps on from there. */
 int ek_batch_resync(ek_batch *b);
+/* Restart the channels with mask[i] != 0 in place from the fields loaded
+ * through their own handles (ek_set_fields): their populations become the
+ * equilibrium of those fields in the buffer the batch steps from next (that
+ * step pulls them, as every step but a batch's first does), their step counts
+ * start over and they step on with the others; the other channels are not
+ * touched.  A run to steady state uses it to send a channel whose start went
+ * wrong back to the cold start without waiting for the rest of the batch.
+ * A restarted channel's next residual compares with its state before the
+ * restart. */
+int ek_batch_restart(ek_batch *b, const uint8_t *mask);
 /* mask (optional, count bytes) and the number of active nodes (optional). */
 int ek_batch_active(const ek_batch *b, uint8_t *mask, int64_t *active_nodes);
 /* ek_residual of every channel: out5 gets 5 doubles per channel (u_x, c+,

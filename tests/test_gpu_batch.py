@@ -83,7 +83,7 @@ def test_batch_bitwise_equals_single_channels(storage, singles, shape, graph):
 
 def test_autotune_keeps_the_bits():
     import ekpnp
-    steps = 6 * (4 + 2) + 11
+    steps = len(ekpnp.Batch.shapes()) * (4 + 2) + 11  # the autotuner runs steps + 2 per shape
     ref = [single(p, i, steps, 10) for p, i in zip(params(ekpnp.STORE_F32), inits())]
     with ekpnp.Batch(params(ekpnp.STORE_F32)) as b:
         for ch, init in zip(b, inits()):
@@ -207,3 +207,47 @@ def test_frozen_channels_keep_their_state_and_others_keep_the_bits():
         b.set_active(np.ones(len(ps), bool))  # even now: rejoin allowed
         b.step(2)
         assert all(np.all(np.isfinite(ch.get_fields(("ux",))["ux"])) for ch in b)
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+def test_restart_in_place_keeps_the_other_channels_bits(storage):
+    """ek_batch_restart gives the masked channels a new start in place: the
+    other channels keep exactly the bits of a batch without the restart, the
+    restarted one holds its new fields right after it, steps on finite with
+    its step count started over, and can be restarted again."""
+    import ekpnp
+    st = {"f32": ekpnp.STORE_F32, "f16": ekpnp.STORE_F16}[storage]
+    ps, ins = params(st), inits()
+    j = 2
+    new = ekpnp.noisy_uniform_state(SPECS[j]["nx"], SPECS[j]["ny"], seed=99)
+
+    def run(restart):
+        with ekpnp.Batch(ps) as b:
+            for ch, init in zip(b, ins):
+                ch.set_fields(**init)
+            b.set_cycle(10)
+            b.init_equilibrium()
+            b.step(20)
+            if restart:
+                b[j].set_fields(**new)
+                mask = np.zeros(len(b), bool)
+                mask[j] = True
+                b.restart(mask)
+                assert np.array_equal(b[j].get_fields(("cp",))["cp"], new["cp"])
+            b.step(24)
+            out = [ch.get_fields(NAMES) for ch in b]
+            if restart:
+                assert b[j].steps == 24 and b[0].steps == 44
+                b[j].set_fields(**new)
+                b.restart(mask)
+                b.step(4)
+                assert all(np.isfinite(v).all() for v in b[j].get_fields(NAMES).values())
+            return out
+
+    plain, restarted = run(False), run(True)
+    for i in range(len(ps)):
+        for k in NAMES:
+            if i == j:
+                assert np.isfinite(restarted[i][k]).all(), k
+            else:
+                assert np.array_equal(plain[i][k], restarted[i][k]), (i, k)

@@ -77,3 +77,70 @@ def test_xreduced_start_needs_widths_that_tile():
         ws.xreduced_start_run(specs, start="cold")
     with pytest.raises(ValueError):
         ws.xreduced_start_run(specs[:1], start="nowhere")
+
+
+class ScriptedBatch:
+    """Stands in for ekpnp.Batch in run_to_steady: channel i's residual at its
+    k-th check since its (re)start is script[i](k, restarted)."""
+
+    def __init__(self, scripts):
+        self.scripts = scripts
+        self.steps = 0
+        self.mask = np.ones(len(scripts), bool)
+        self.since = np.zeros(len(scripts), int)      # checks since the channel's start
+        self.restarts = []
+        self.was_restarted = np.zeros(len(scripts), bool)
+
+    def __len__(self):
+        return len(self.scripts)
+
+    def sync(self):
+        pass
+
+    def step(self, k):
+        self.steps += k
+
+    @property
+    def active(self):
+        return self.mask.copy(), int(self.mask.sum())
+
+    def set_active(self, mask):
+        self.mask = np.asarray(mask, bool).copy()
+
+    def residual(self, check):
+        out = np.zeros((len(self.scripts), 5))
+        for i, f in enumerate(self.scripts):
+            out[i, 4] = f(self.since[i], self.was_restarted[i])
+            if self.mask[i]:
+                self.since[i] += 1
+        return out
+
+    def restart(self, idx):
+        self.restarts.append(list(idx))
+        for i in idx:
+            self.was_restarted[i] = True
+            self.since[i] = 0
+            self.mask[i] = True
+
+
+def test_run_to_steady_restarts_judged_channels_in_place():
+    """Channels whose residual rises between the judged checks, or that go
+    non-finite, are restarted once, in place, and reach steady state in the
+    same run; the check right after a restart is not judged; the others are
+    untouched."""
+    from ekpnp import warmstart as ws
+    decay = lambda k, r: 10.0 ** (-2 - k)                       # converges at its 7th check
+    rise = lambda k, r: 10.0 ** (-2 - k) if r else 1e-3 * (k + 1)   # rises until restarted
+    nan = lambda k, r: 10.0 ** (-2 - k) if r else float("nan")      # diverges until restarted
+    b = ScriptedBatch([decay, rise, nan])
+    info = ws.run_to_steady(b, tol=1e-8, check=2, max_steps=200, judge=(1, 3),
+                            restart=b.restart)
+    assert b.restarts == [[2], [1]]                # the non-finite one at once, the rising one at check 3
+    assert info["restarted"].tolist() == [False, True, True]
+    assert np.all(info["steps"] > 0) and not info["diverged"].any()
+    assert info["steps"][0] < info["steps"][2] < info["steps"][1]
+    # without restart the judged channels are frozen and reported as rising
+    b2 = ScriptedBatch([decay, rise, nan])
+    info2 = ws.run_to_steady(b2, tol=1e-8, check=2, max_steps=200, judge=(1, 3))
+    assert b2.restarts == [] and info2["rising"].tolist() == [False, True, True]
+    assert info2["steps"][0] > 0 and info2["steps"][1] < 0 and info2["steps"][2] < 0
