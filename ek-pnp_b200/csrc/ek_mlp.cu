@@ -3,11 +3,13 @@
 // GPU by hand-written kernels.
 //
 //   GEMMs      C = A B^T on the 5th-generation tensor cores: BF16 operands
-//              staged in shared memory (K-major, no swizzle), tcgen05.mma
-//              issued by one thread into an FP32 accumulator in tensor memory,
-//              completion through tcgen05.commit on an mbarrier (bounded wait),
-//              tcgen05.ld into registers for a fused epilogue (bias, SiLU,
-//              SiLU derivative, BF16 and transposed BF16 stores).
+//              copied asynchronously into a 4-slot ring of shared-memory
+//              stages (K-major, no swizzle), tcgen05.mma issued by one thread
+//              into an FP32 accumulator in tensor memory as each K chunk
+//              lands, completion through tcgen05.commit on each slot's
+//              mbarrier (bounded waits), tcgen05.ld into registers for a fused
+//              epilogue (bias, SiLU, SiLU derivative, BF16 and transposed
+//              BF16 stores).
 //   training   per iteration: batch gather, 4 forward GEMMs, MSE loss and its
 //              gradient, 3 backward-data and 4 weight-gradient GEMMs, bias
 //              gradients, Adam on FP32 master weights, BF16 weight casts --
@@ -65,11 +67,37 @@ __device__ __forceinline__ float silu_grad(float z) {
 }
 
 // One 128 x nt tile of C = A B^T per CTA of 128 threads.
+//
+// K is cut into chunks of KC; chunk c is staged in ring slot c % STAGES
+// (A: TM x KC, B: nt x KC, BF16, the canonical K-major layout).  The copies
+// are 16-byte asynchronous copies (cp.async.cg, global -> shared) issued by
+// all threads, one commit group per chunk: the first STAGES chunks are all
+// in flight before the first MMA, and a slot is refilled as soon as the MMAs
+// that read it have completed, so loads of later chunks overlap the MMAs of
+// earlier ones.  One thread issues each chunk's tcgen05.mma instructions and
+// commits them to the slot's mbarrier; every slot has at most one
+// uncompleted commit at a time, so a wait by parity is unambiguous.
+constexpr int STAGES = 4;
+constexpr size_t STAGE_A = (size_t)TM * KC * 2, STAGE_BYTES = STAGE_A + (size_t)NT_MAX * KC * 2;
+constexpr size_t GEMM_SMEM = STAGES * STAGE_BYTES;
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(ek::tc::smem_u32(smem)), "l"(gmem) : "memory");
+}
+// Wait until at most n of this thread's commit groups are pending (n < STAGES).
+__device__ __forceinline__ void cp_async_wait_pending(int n) {
+    switch (n) {
+        case 0: asm volatile("cp.async.wait_group 0;" ::: "memory"); break;
+        case 1: asm volatile("cp.async.wait_group 1;" ::: "memory"); break;
+        case 2: asm volatile("cp.async.wait_group 2;" ::: "memory"); break;
+        default: asm volatile("cp.async.wait_group 3;" ::: "memory"); break;
+    }
+}
+
 template <int EPI>
 __global__ void __launch_bounds__(128) mlp_gemm(const GemmArgs g) {
-    __shared__ __align__(1024) uint8_t sa[TM * KC * 2];
-    __shared__ __align__(1024) uint8_t sb[NT_MAX * KC * 2];
-    __shared__ __align__(8) uint64_t bar;
+    extern __shared__ __align__(1024) uint8_t stage_mem[];
+    __shared__ __align__(8) uint64_t bar[STAGES];
     __shared__ uint32_t tmem_base;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m0 = blockIdx.x * TM, n0 = blockIdx.y * g.nt;
@@ -78,7 +106,7 @@ __global__ void __launch_bounds__(128) mlp_gemm(const GemmArgs g) {
         ek::tc::tmem_relinquish();
     }
     if (tid == 0) {
-        ek::tc::mbar_init(&bar, 1);
+        for (int b = 0; b < STAGES; ++b) ek::tc::mbar_init(&bar[b], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     ek::tc::fence_before_sync();
@@ -86,45 +114,72 @@ __global__ void __launch_bounds__(128) mlp_gemm(const GemmArgs g) {
     ek::tc::fence_after_sync();
     const uint32_t tmem = tmem_base;
     const uint32_t idesc = ek::tc::idesc_bf16_f32(TM, g.nt);
-    uint32_t phase = 0;
-    bool failed = false;
-    for (int k0 = 0; k0 < g.k; k0 += KC) {
-        const int kk = min(KC, g.k - k0);  // a multiple of 16
-        const int vpr = kk >> 3;           // 16-byte vectors per row
+    const int nk = (g.k + KC - 1) / KC;
+    // copies of chunk c into its ring slot
+    auto load = [&](int c) {
+        uint8_t *sa = stage_mem + (size_t)(c % STAGES) * STAGE_BYTES, *sb = sa + STAGE_A;
+        const int k0 = c * KC;
+        const int vpr = min(KC, g.k - k0) >> 3;  // 16-byte vectors per row (kk a multiple of 16)
         for (int v = tid; v < TM * vpr; v += 128) {
-            const int r = v / vpr, c = v - r * vpr;
-            const uint4 val = *reinterpret_cast<const uint4 *>(g.a + (size_t)(m0 + r) * g.lda + k0 + c * 8);
-            *reinterpret_cast<uint4 *>(sa + ((r >> 3) * (KC / 8) + c) * 128 + (r & 7) * 16) = val;
+            const int r = v / vpr, cc = v - r * vpr;
+            cp_async16(sa + ((r >> 3) * (KC / 8) + cc) * 128 + (r & 7) * 16, g.a + (size_t)(m0 + r) * g.lda + k0 + cc * 8);
         }
         for (int v = tid; v < g.nt * vpr; v += 128) {
-            const int r = v / vpr, c = v - r * vpr;
-            const uint4 val = *reinterpret_cast<const uint4 *>(g.b + (size_t)(n0 + r) * g.ldb + k0 + c * 8);
-            *reinterpret_cast<uint4 *>(sb + ((r >> 3) * (KC / 8) + c) * 128 + (r & 7) * 16) = val;
+            const int r = v / vpr, cc = v - r * vpr;
+            cp_async16(sb + ((r >> 3) * (KC / 8) + cc) * 128 + (r & 7) * 16, g.b + (size_t)(n0 + r) * g.ldb + k0 + cc * 8);
         }
-        ek::tc::fence_async_smem();
-        __syncthreads();
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    uint32_t phase = 0;  // bit b: parity of slot b's next completion
+    uint32_t open = 0;   // bit b: slot b has a commit not yet waited for
+    const int pre = min(nk, STAGES);
+    for (int c = 0; c < pre; ++c) load(c);
+    bool failed = false;
+    for (int i = 0; i < nk && !failed; ++i) {
+        const int st = i % STAGES;
+        cp_async_wait_pending(min(nk - 1 - i, STAGES - 1));  // chunk i's copies (this thread's) have landed
+        ek::tc::fence_async_smem();                            // visible to the tensor cores
+        __syncthreads();                                       // every thread's copies of chunk i
         if (tid == 0) {
             ek::tc::fence_after_sync();
-            const uint32_t a0 = ek::tc::smem_u32(sa), b0 = ek::tc::smem_u32(sb);
+            const uint32_t a0 = ek::tc::smem_u32(stage_mem + (size_t)st * STAGE_BYTES), b0 = a0 + (uint32_t)STAGE_A;
+            const int kk = min(KC, g.k - i * KC);
             for (int kq = 0; kq < kk / 16; ++kq) {
                 // 16 K-elements = two core matrices along K
                 const uint64_t ad = ek::tc::smem_desc(a0 + kq * 256, 128, (KC / 8) * 128);
                 const uint64_t bd = ek::tc::smem_desc(b0 + kq * 256, 128, (KC / 8) * 128);
-                ek::tc::mma_bf16(tmem, ad, bd, idesc, (k0 > 0 || kq > 0) ? 1u : 0u);
+                ek::tc::mma_bf16(tmem, ad, bd, idesc, (i > 0 || kq > 0) ? 1u : 0u);
             }
-            ek::tc::mma_commit(&bar);
+            ek::tc::mma_commit(&bar[st]);
         }
-        const bool ok = ek::tc::mbar_wait_bounded(&bar, phase, g.wait_cycles);
-        phase ^= 1;
-        failed = __syncthreads_or(!ok) != 0;  // also: the tiles may be overwritten
-        ek::tc::fence_after_sync();
-        if (failed) break;
+        open |= 1u << st;
+        if (i + STAGES < nk) {
+            // the slot is refilled once the MMAs that read it have completed
+            const bool ok = ek::tc::mbar_wait_bounded(&bar[st], (phase >> st) & 1u, g.wait_cycles);
+            failed = __syncthreads_or(!ok) != 0;
+            if (!failed) {
+                phase ^= 1u << st;
+                open &= ~(1u << st);
+                ek::tc::fence_after_sync();
+                load(i + STAGES);
+            }
+        }
     }
+    // the accumulator is complete once every open commit has arrived (the
+    // last one tracks all MMAs issued before it); after a failed wait, MMAs
+    // still in flight get one more wait at the default bound before the
+    // tensor memory is freed
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    for (int b = 0; b < STAGES; ++b) {
+        if (!((open >> b) & 1u)) continue;
+        if (!failed && ek::tc::mbar_wait_bounded(&bar[b], (phase >> b) & 1u, g.wait_cycles)) continue;
+        failed = true;
+        ek::tc::mbar_wait_bounded(&bar[b], (phase >> b) & 1u, ek::tc::WAIT_CYCLES_DEFAULT);
+    }
+    failed = __syncthreads_or(failed) != 0;
+    ek::tc::fence_after_sync();
     if (failed) {
         if (tid == 0) atomicOr(g.err, 1);
-        // MMAs still in flight get one more wait, at the default bound
-        // whatever the pipeline's, before the tensor memory is freed
-        ek::tc::mbar_wait_bounded(&bar, phase, ek::tc::WAIT_CYCLES_DEFAULT);
     } else {
         const int row = m0 + warp * 32 + lane;
         const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
@@ -303,10 +358,23 @@ int cuda_err(cudaError_t e, const char *what) {
         if (e_ != cudaSuccess) return cuda_err(e_, what); \
     } while (0)
 
+// The GEMM's ring of stages is dynamic shared memory above the 48 KB
+// default: allow it for every epilogue on the current device, before any
+// launch (and outside any stream capture).
+cudaError_t gemm_set_attributes() {
+    const void *fns[] = {(const void *)mlp_gemm<EPI_F32>, (const void *)mlp_gemm<EPI_FWD_HIDDEN>,
+                         (const void *)mlp_gemm<EPI_FWD_OUT>, (const void *)mlp_gemm<EPI_BWD_HIDDEN>};
+    for (const void *f : fns) {
+        const cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 template <int EPI>
 cudaError_t gemm(const GemmArgs &a, cudaStream_t s) {
     const dim3 grid(a.m / TM, a.n / a.nt);
-    mlp_gemm<EPI><<<grid, 128, 0, s>>>(a);
+    mlp_gemm<EPI><<<grid, 128, GEMM_SMEM, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -450,6 +518,7 @@ extern "C" {
 int ek_mlp_create(int32_t batch, uint64_t seed, ek_mlp **out) {
     if (!out || batch <= 0 || batch % TM) return ek::ctx_fail(EK_ERR_INVALID, "batch must be a positive multiple of 128");
     *out = nullptr;
+    EK_MCUDA(gemm_set_attributes(), "GEMM attributes");
     ek_mlp *q = new ek_mlp();
     q->B = batch;
     q->rng.seed(seed);
@@ -799,6 +868,7 @@ int ek_gemm_bf16(const uint16_t *a, int32_t lda, const uint16_t *b, int32_t ldb,
         EK_MCUDA(cudaMalloc(&err, 4), "error word");
         EK_MCUDA(cudaMemset(err, 0, 4), "error word");
     }
+    EK_MCUDA(gemm_set_attributes(), "GEMM attributes");
     GemmArgs g = args((const bf16 *)a, lda, (const bf16 *)b, ldb, m, n, k, err);
     g.c = c;
     g.ldc = ldc;
