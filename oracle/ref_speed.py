@@ -9,10 +9,9 @@ Usage (on a GPU, after oracle/ref_build.py built both binaries):
     python oracle/ref_speed.py [--pb] [case ...] > speed.json
 Prints one JSON object per case: MLUPS, GPU and clock runtimes of each
 binary.  The reference's MLUPS counts NSTEPS = steps - 1 steps (main.cu:244).
---pb starts from the Poisson-Boltzmann state (the library's Newton form)
-instead of the case's noisy uniform state: a state that stays finite, since
-the noisy start at zeta = -4 diverges within ~100 steps in both codes and
-FP64 arithmetic on non-finite values takes slow paths (divisions).
+--pb starts from the Poisson-Boltzmann state (the library's Newton form,
+the steady double layers a long run spends its time near) instead of the
+case's noisy uniform state.
 """
 from __future__ import annotations
 
